@@ -1,0 +1,363 @@
+"""Benchmark of the KerrTrace hot path on B200.
+
+One step = one 1920x1080 frame of the c2 scene (a = 0.998, r_obs 100 M, inclination 85 deg,
+tolerance 1e-6, up to 20000 DP5(4) steps per ray, FBM-modulated Novikov-Thorne disk, bloom
+radius 24, ACES + sRGB): the trace kernel plus the post-processing kernel.
+
+  value   Mrays/s over all ranks, device-timed (CUDA events around each step on the launch
+          stream; L2 flushed between steps by writing a 256 MiB buffer outside the timed events)
+  e2e     the same metric through the public renderer API (kt_renderer_submit_render +
+          ready_frame + finish_frame): per frame the camera goes host -> device as launch
+          arguments and the 0x00RRGGBB frame plus its LUT error word come back into pinned
+          host memory; wall-clock per frame after a device synchronise
+  roofline  FP32 work of the trace kernel (counted RHS evaluations / attempts / steps x the
+          static op counts in kerrtrace_b200/flops.py) / its event-timed duration, against the
+          FP32 FMA peak at the SM clock sampled during the run (148 SMs x 128 lanes x 2 flops)
+  cpu_baseline  the CPU oracle (f64 restatement, all host cores) on a strided sample of the
+          same frame
+
+--impl reference runs the reference's own cuda/kernel.cu (compiled from source into
+oracle/_ref) with the launch sequence of src/renderer/mod.rs: trace_kernel, bloom_horizontal,
+post_process, image copy to pinned host memory.
+
+Multi-GPU (torchrun): every rank renders its own frame of the same scene seen from a different
+azimuth (the spacetime is axisymmetric, so every rank has the same work): weak scaling, no
+data-path collective; the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = Path(f"/tmp/kt_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path.exists():
+            for line in self.path.read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+            self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()),
+                "samples": len(rows)}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_camera(kt, workloads, name, rank, world):
+    cfg, cam = workloads.scene(name)
+    if world > 1 and rank > 0:
+        r = math.sqrt(sum(c * c for c in cam.cam_pos))
+        incl = math.degrees(math.acos(cam.cam_pos[1] / r))
+        fov = 2 * math.degrees(math.atan(cam.fov_scale))
+        cam = kt.orbit_camera(r, incl, fov, azimuth_deg=360.0 * rank / world)
+    return cfg, cam
+
+
+def cpu_baseline(cfg, cam, budget_s: float) -> dict:
+    """The CPU oracle (f64, reference semantics, all host cores) on a strided pixel sample."""
+    import numpy as np
+
+    import oracle
+    threads = os.cpu_count() or 1
+    sc = oracle.Scene(cfg, cam, tex_mode=1)
+    n = cfg.width * cfg.height
+    stride = 4096
+    t = 0.0
+    while True:
+        pix = np.arange(0, n, stride, dtype=np.int64)
+        t0 = time.perf_counter()
+        sc.render(2, pixels=pix, threads=threads)
+        t = time.perf_counter() - t0
+        if t > budget_s / 4 or stride <= 16:
+            break
+        stride = max(16, int(stride * max(0.1, t / (budget_s / 2))) if t > 0 else stride // 8)
+    rays = len(pix) * cfg.spp
+    return {"value": rays / t / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"f64 oracle, every {stride}th pixel of the {cfg.width}x{cfg.height} frame "
+                      f"({len(pix)} pixels x {cfg.spp} spp) in {t:.2f} s"}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import kerrtrace_b200 as kt
+    from kerrtrace_b200 import flops, workloads
+
+    cfg, cam = rank_camera(kt, workloads, args.workload, rank, world)
+    sched = kt.SCHED_WAVEFRONT if args.schedule == "wavefront" else kt.SCHED_PLAIN
+    ctx = kt.Context(cfg, local)
+    n = cfg.width * cfg.height
+    hdr = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    img = torch.zeros(n, dtype=torch.int32, device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    stats = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), stream, sched)
+    work = flops.trace_flops(stats)
+
+    def step():
+        err.zero_()
+        ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), stream, sched)
+        ctx.post_fused(hdr.data_ptr(), img.data_ptr(), stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        for e0, e1, e2 in ev:
+            flush.fill_(1.0)
+            err.zero_()
+            e0.record()
+            ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), stream, sched)
+            e1.record()
+            ctx.post_fused(hdr.data_ptr(), img.data_ptr(), stream)
+            e2.record()
+        torch.cuda.synchronize()
+        barrier(world)
+    clocks = clk.summary()
+    t_steps = [a.elapsed_time(c) for a, _, c in ev]
+    t_trace = [a.elapsed_time(b) for a, b, _ in ev]
+    t_post = [b.elapsed_time(c) for _, b, c in ev]
+    total_ms = max_over_ranks(sum(t_steps), world)
+    rays_all = n * cfg.spp * world * args.steps
+    value = rays_all / (total_ms / 1e3) / 1e6
+
+    # end to end through the renderer API (host buffers)
+    rend = kt.Renderer(cfg, local)
+    rend.set_schedule(sched)
+    cam_args = (list(cam.cam_pos), list(cam.fwd), list(cam.rgt), list(cam.up), cam.fov_scale)
+
+    def frame():
+        assert rend.submit_render(*cam_args)
+        rend.wait()
+        idx, data = rend.ready_frame()
+        rend.finish_frame(idx)
+        return data
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        frame()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    rend.close()
+    e2e = {"value": rays_all / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 52,
+           "d2h_bytes_per_step": n * 4 + 8, "ms_per_step": e2e_s * 1e3 / args.steps}
+
+    trace_ms = sum(t_trace) / len(t_trace)
+    achieved = work / (trace_ms / 1e3) / 1e12
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    mhz = clocks.get("sm_mhz") or 1965.0
+    peak = sms * flops.FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+    roofline = {"bound": "fp32", "kernel": "trace_wavefront_kernel" if sched else "trace_plain_kernel",
+                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4),
+                "peak_source": f"FP32 FMA peak at the sampled median SM clock ({mhz:.0f} MHz): "
+                               f"{sms} SMs x 128 lanes x 2 flops",
+                "traffic": None, "trace_ms": round(trace_ms, 4),
+                "post_ms": round(sum(t_post) / len(t_post), 4),
+                "work": {"rays": int(stats.rays), "steps": int(stats.steps), "attempts": int(stats.attempts),
+                         "rhs_evals": int(stats.rhs_evals), "frozen_rays": int(stats.frozen_rays),
+                         "flops": work}}
+    line = {
+        "metric": "Mrays/s 1080p (c2 scene, trace + post)", "value": round(value, 3), "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, camera rays)",
+        "config": {"workload": f"{args.workload}: {cfg.width}x{cfg.height}, a={cfg.spin:.3f}, tol={cfg.tolerance:g}, "
+                               f"max_steps={cfg.max_steps}, spp={cfg.spp}, bloom r={cfg.bloom_radius:g}",
+                   "schedule": args.schedule, "mode": "reference semantics (drop-in)", "precision": "fp32",
+                   "l2": "flushed between steps (256 MiB write outside the timed events)",
+                   "parallelism": f"replica frames x{world}"},
+        "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": 2 * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, cam, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def run_reference(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import kerrtrace_b200 as kt
+    import oracle
+    from kerrtrace_b200 import workloads
+
+    if rank != 0:
+        return
+    cfg, cam = workloads.scene(args.workload)
+    if not oracle.ref_lib_path(args.workload).exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/libktref_{args.workload}.so not built"}))
+        return
+    p = kt.build_kerr_params(cfg)
+    bb = kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start, cfg.wavelength_end,
+                                   cfg.wavelength_step)
+    disk = kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)
+    ref = oracle.RefKernel(args.workload)
+    ref.setup(p, bb, disk)
+    n = cfg.width * cfg.height
+    hdr = torch.zeros((n, 4), device="cuda")
+    bloom = torch.zeros((n, 4), device="cuda")
+    img = torch.zeros(n, dtype=torch.int32, device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    host_img = torch.zeros(n, dtype=torch.int32).pin_memory()
+    host_err = torch.zeros(2, dtype=torch.int32).pin_memory()
+    radius = int(math.ceil(np.float32(cfg.bloom_radius))) if cfg.bloom_radius > 0 else 0
+    sigma = float(np.float32(cfg.bloom_radius) / np.float32(3.0))
+    active = int(bool(cfg.bloom_enabled) and radius > 0 and cfg.bloom_intensity > 0)
+
+    def frame():  # src/renderer/mod.rs:543-603
+        err.zero_()
+        ref.trace(hdr.data_ptr(), cfg, cam, cfg.lut_max_temp, err.data_ptr(), p.disk_inner)
+        host_err.copy_(err, non_blocking=True)
+        if active:
+            ref.bloom(hdr.data_ptr(), bloom.data_ptr(), cfg, radius, sigma, active)
+        ref.post(hdr.data_ptr(), bloom.data_ptr(), img.data_ptr(), cfg, radius, sigma, cfg.bloom_intensity, active)
+        host_img.copy_(img, non_blocking=True)
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    evs = []
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            frame()
+            e1.record()
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    rays = n * cfg.spp * args.steps
+    value = rays / (dev_ms / 1e3) / 1e6
+    line = {"impl": "reference", "metric": "Mrays/s 1080p (c2 scene, trace + post)", "value": round(value, 3),
+            "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, camera rays)",
+            "config": {"workload": f"{args.workload}: {cfg.width}x{cfg.height}",
+                       "implementation": "reference cuda/kernel.cu compiled from source for sm_100a "
+                                         "(-use_fast_math, the reference's #define header), mod.rs launch sequence"},
+            "e2e": {"value": round(rays / wall / 1e6, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 52,
+                    "d2h_bytes_per_step": n * 4 + 8},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": 0, "kind": "reference",
+                             "sample": "the reference's path has no CPU implementation: this line times its GPU "
+                                       "kernels (oracle/_ref) on the same B200"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    ref.close()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,242 @@
+/*
+ * kerrtrace.h — C ABI of the B200-native KerrTrace geodesic hot path.
+ *
+ * The reference (DamoyY/KerrTrace) JIT-compiles cuda/kernel.cu with NVRTC, uploads
+ * `__constant__ KerrParams c_params`, builds two LUT textures and launches three kernels per
+ * frame from Rust (src/renderer/{init,mod,texture,utils,blackbody}.rs).  This header is the
+ * drop-in for that layer: plain C types, caller-owned buffers, stream-ordered calls, status
+ * codes instead of panics.  Each entry point names the reference item it replaces.
+ *
+ * Conventions
+ *  - Every `stream` argument is a `cudaStream_t` passed as `void*` (NULL = legacy default
+ *    stream, the one cudarc's `context.default_stream()` uses, src/renderer/mod.rs:474).
+ *  - Device pointers are marked `dev`; host pointers `host`.  The caller owns every output
+ *    buffer.  A context owns its LUT textures and the small scratch words of the wavefront
+ *    tracer; calls on one context must be ordered on one stream at a time.
+ *  - No call synchronises unless its comment says so.  Device-side failures (LUT overflow,
+ *    non-finite input) are reported through the 2 x u32 error word exactly like the
+ *    reference's `lut_error_flag` (cuda/kernel.cu:3-9): word[0] = 1 on the first failure,
+ *    word[1] = the f32 bits of the offending temperature.
+ *  - No exception or abort crosses this boundary.  On failure a call returns a status and
+ *    `kt_last_error()` holds a message for the calling thread.
+ */
+#ifndef KERRTRACE_H
+#define KERRTRACE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KT_ABI_VERSION 1
+
+typedef enum kt_status {
+    KT_OK = 0,
+    KT_ERR_INVALID_ARG = 1,   /* bad config / pointer / size (reference: anyhow! in utils.rs, init.rs) */
+    KT_ERR_CUDA = 2,          /* a CUDA runtime call failed (reference: cudarc DriverError) */
+    KT_ERR_LUT_OVERFLOW = 3,  /* colour temperature above lut_max_temp (mod.rs:630-635) */
+    KT_ERR_NOT_READY = 4,     /* frame not complete yet (mod.rs:620 returns Ok(None)) */
+    KT_ERR_QUEUE_ORDER = 5,   /* finish_frame out of order (mod.rs:646-650) */
+    KT_ERR_NO_DEVICE = 6,     /* no CUDA device / library built without one */
+    KT_ERR_UNSUPPORTED = 7,   /* option not available in this build */
+    KT_ERR_TIMEOUT = 8        /* a bounded device wait gave up */
+} kt_status;
+
+/* Integration semantics.  KT_MODE_REF reproduces the reference kernel exactly, including its
+ * documented quirks (linear-guess crossing root, H-scaled tolerance that reaches zero near the
+ * hole, always-jittered pixel samples).  KT_MODE_SPEC follows the stated physics instead:
+ * Newton/bisection crossing root on the dense output, tolerance never below `tolerance`,
+ * pixel-centre samples at spp = 1, seeded/phased FBM and a luminance bloom threshold. */
+typedef enum kt_mode { KT_MODE_REF = 0, KT_MODE_SPEC = 1 } kt_mode;
+
+/* Arithmetic of the geodesic integration.  FP32 is the reference's arithmetic.  MIXED keeps
+ * FP32 for the bulk and uses FP64 for the state update / error norm inside 1.5 x the photon
+ * orbit radius or near the horizon, the null-constraint renormalisation of p and the crossing
+ * solve.  FP64 runs the whole integration in double. */
+typedef enum kt_precision { KT_PREC_FP32 = 0, KT_PREC_MIXED = 1, KT_PREC_FP64 = 2 } kt_precision;
+
+/* Scheduling of the trace kernel. */
+typedef enum kt_schedule {
+    KT_SCHED_PLAIN = 0,     /* one thread per pixel on a 2D grid of block_dim tiles (kernel.cu:88) */
+    KT_SCHED_WAVEFRONT = 1  /* persistent kernel, per-lane refill from a device work queue */
+} kt_schedule;
+
+/*
+ * Full configuration.  Field names follow the reference's config.yaml / serde structs
+ * (src/main.rs:15-122); values that the reference bakes into `#define`s
+ * (src/renderer/utils.rs:121-163) are runtime values here.  Use kt_config_default() for the
+ * reference's config.yaml values.
+ */
+typedef struct kt_config {
+    /* window (main.rs:28-32) */
+    uint32_t width;
+    uint32_t height;
+    /* renderer (main.rs:50-54) */
+    uint32_t block_dim[2];
+    /* bloom (main.rs:56-60) */
+    int32_t bloom_enabled;
+    float bloom_intensity;
+    float bloom_radius;
+    /* blackbody (main.rs:68-74) */
+    uint32_t lut_size;
+    float lut_max_temp;
+    float wavelength_start;
+    float wavelength_end;
+    float wavelength_step;
+    /* cuda (main.rs:76-78).  Must be 1: the kernels are built with -use_fast_math. */
+    int32_t use_fast_math;
+    /* kernel (main.rs:88-122) */
+    uint32_t spp;
+    float exposure_scale;
+    uint32_t sky_grid_divisions;
+    float sky_line_thickness;
+    float sky_intensity;
+    float spin;
+    float mass;
+    float disk_outer_radius;
+    float disk_temperature_scale;
+    float initial_step;
+    float tolerance;
+    uint32_t max_steps;
+    uint32_t max_attempts;
+    float transmittance_cutoff;
+    float horizon_epsilon;
+    float escape_radius;
+    /* disk_noise (main.rs:80-86) */
+    int32_t noise_enabled;
+    float noise_scale;
+    float noise_strength;
+    float noise_winding;
+    uint32_t noise_detail;
+    /* extensions (no reference counterpart; zero = reference behaviour) */
+    int32_t mode;            /* kt_mode */
+    int32_t precision;       /* kt_precision */
+    uint32_t noise_seed;     /* KT_MODE_SPEC only: XORed into the FBM lattice hash */
+    float noise_phase;       /* KT_MODE_SPEC only: added to the disk azimuth */
+    float bloom_threshold;   /* KT_MODE_SPEC only: bloom source = max(L - threshold, 0)/L * hdr */
+    float photon_zone_factor;/* KT_PREC_MIXED: FP64 zone radius = factor * photon orbit radius (0 = 1.5) */
+} kt_config;
+
+/* Mirror of the reference's `KerrParams` (cuda/kerr_math.cuh:3-9, src/renderer/init.rs:15-33). */
+typedef struct kt_kerr_params {
+    float a, m, aa, inv_m, a_norm, rh, disk_inner;
+    float inv_w_2, inv_h_2, aspect_ratio;
+    float disk_noise_scale, disk_noise_strength, disk_noise_winding;
+    int32_t disk_noise_enabled, disk_noise_detail;
+} kt_kerr_params;
+
+/* Camera of one frame: the arguments of CudaRenderer::submit_render (mod.rs:513-520). */
+typedef struct kt_camera {
+    float cam_pos[3];
+    float fwd[3];
+    float rgt[3];
+    float up[3];
+    float fov_scale;  /* tan(fov / 2), src/app.rs:163 */
+} kt_camera;
+
+/* Per-launch statistics of a trace (optional; pass NULL to skip counting). */
+typedef struct kt_trace_stats {
+    uint64_t rays;
+    uint64_t steps;        /* committed integration steps */
+    uint64_t attempts;     /* DP5(4) attempts (accepted + rejected) */
+    uint64_t rhs_evals;    /* Hamiltonian right-hand-side evaluations */
+    uint64_t frozen_rays;  /* rays retired early because their state became NaN */
+    uint64_t fp64_steps;   /* steps taken with the FP64 update (KT_PREC_MIXED) */
+} kt_trace_stats;
+
+typedef struct kt_context kt_context;
+typedef struct kt_renderer kt_renderer;
+
+/* ---- status ---------------------------------------------------------------------------- */
+const char* kt_status_str(kt_status s);
+/* Message of the last failure on the calling thread ("" if none). */
+const char* kt_last_error(void);
+int kt_abi_version(void);
+
+/* ---- host precompute (CPU only, no device needed) ---------------------------------------- */
+/* Defaults of the reference's config.yaml (config.yaml:1-67). */
+kt_status kt_config_default(kt_config* cfg);
+/* build_kerr_params (src/renderer/utils.rs:53-113): rh, prograde ISCO, 2/W, 2/H, W/H. */
+kt_status kt_build_kerr_params(const kt_config* cfg, kt_kerr_params* out);
+/* calc_isco (src/renderer/utils.rs:11-20), f32 arithmetic as the reference host. */
+float kt_calc_isco(float a_norm, int prograde, float mass);
+/* generate_blackbody_lut (src/renderer/blackbody.rs:56-124): `size` RGBA f32 rows on a linear
+ * temperature grid [0, max_temp].  out_rgba holds size*4 floats. */
+kt_status kt_generate_blackbody_lut(uint32_t size, float max_temp, float wavelength_start,
+                                    float wavelength_end, float wavelength_step, float* out_rgba);
+/* generate_disk_temperature_lut (src/renderer/utils.rs:172-201): f^(1/4) of the
+ * Novikov-Thorne / Page-Thorne flux factor on `size` radii in [disk_inner, disk_outer]. */
+kt_status kt_generate_disk_lut(const kt_kerr_params* params, float disk_outer, uint32_t size,
+                               float* out);
+/* build_cuda_defines (src/renderer/utils.rs:121-163): the `#define` header text the reference
+ * prepends to kernel.cu.  Writes a NUL-terminated string; *len gets its length. */
+kt_status kt_build_defines(const kt_config* cfg, char* buf, size_t cap, size_t* len);
+/* calculate_camera_basis (src/math.rs:3-14): forward from yaw/pitch in degrees, right =
+ * forward x (0,1,0), up = right x forward, each normalised (glam f32 arithmetic). */
+kt_status kt_camera_basis(float yaw_deg, float pitch_deg, float fwd[3], float rgt[3], float up[3]);
+/* fov_scale = tan(fov.to_radians() / 2) (src/app.rs:163). */
+float kt_fov_scale(float fov_deg);
+/* validate_bloom_settings (src/renderer/init.rs:43-73). */
+kt_status kt_validate_bloom(const kt_config* cfg, int32_t* enabled, float* intensity,
+                            float* radius, int32_t* radius_int);
+
+/* ---- device context: replaces build_textures + build_cuda_kernels (init.rs:74-140) -------- */
+/* Builds KerrParams and both LUTs on the host, uploads the LUTs as 1D linear-filtered,
+ * normalised, clamped textures (texture.rs:86-202) and keeps the scene parameters. */
+kt_status kt_context_create(const kt_config* cfg, int device, kt_context** out);
+/* Same, with caller-supplied LUTs (host arrays: bb_rgba lut_n*4 floats, disk lut_n floats). */
+kt_status kt_context_create_with_luts(const kt_config* cfg, int device, const float* bb_rgba,
+                                      const float* disk, uint32_t lut_n, kt_context** out);
+void kt_context_destroy(kt_context* ctx);
+/* Copies out the derived KerrParams the context uses. */
+kt_status kt_context_params(const kt_context* ctx, kt_kerr_params* out);
+
+/* ---- per-frame kernels: replace the three launches of submit_render (mod.rs:547-600) ------ */
+/* trace_kernel (cuda/kernel.cu:88-142): writes W*H float4 (r,g,b,1) HDR, row-major.
+ * hdr_out: dev float[4*W*H]; err_word: dev uint32[2] (not cleared here, like the reference,
+ * which clears it with memset_zeros before the launch, mod.rs:544-546). */
+kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
+                   float* hdr_out, uint32_t* err_word);
+/* Same as kt_trace, plus per-launch counters (synchronises the stream to read them). */
+kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam,
+                           int32_t schedule, float* hdr_out, uint32_t* err_word,
+                           kt_trace_stats* stats);
+/* bloom_horizontal (cuda/kernel.cu:144-173): dev float4 hdr -> dev float4 bloom. */
+kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom);
+/* post_process (cuda/kernel.cu:175-251): vertical blur + composite + ACES + sRGB + pack to
+ * 0x00RRGGBB.  bloom may be NULL when bloom is inactive. */
+kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const float* bloom,
+                          uint32_t* image_out);
+/* Both post passes in one kernel (no bloom buffer round trip); same output bits as
+ * kt_bloom_horizontal followed by kt_post_process. */
+kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_t* image_out);
+
+/* ---- CudaRenderer mirror (src/renderer/mod.rs:469-687) ------------------------------------ */
+/* CudaRenderer::new (mod.rs:470-511): context + two frame buffers with pinned host images. */
+kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out);
+/* CudaRenderer::submit_render (mod.rs:513-612).  *submitted = 0 when both frames are in
+ * flight (the reference returns Ok(false)). */
+kt_status kt_renderer_submit_render(kt_renderer* r, const float cam_pos[3], const float fwd[3],
+                                    const float rgt[3], const float up[3], float fov_scale,
+                                    int32_t* submitted);
+/* CudaRenderer::ready_frame (mod.rs:614-644).  Returns KT_ERR_NOT_READY when no frame is
+ * complete, KT_ERR_LUT_OVERFLOW (and *overflow_temp) when the frame's error word was set. */
+kt_status kt_renderer_ready_frame(kt_renderer* r, uint32_t* index, const uint32_t** data,
+                                  float* overflow_temp);
+/* CudaRenderer::finish_frame (mod.rs:646-654). */
+kt_status kt_renderer_finish_frame(kt_renderer* r, uint32_t index);
+/* Blocks until every submitted frame is complete (no reference counterpart; used by hosts
+ * that render headless). */
+kt_status kt_renderer_wait(kt_renderer* r);
+/* Selects the trace schedule used by submit_render (default KT_SCHED_WAVEFRONT). */
+kt_status kt_renderer_set_schedule(kt_renderer* r, int32_t schedule);
+/* The device HDR buffer of a frame (valid until the frame is resubmitted). */
+kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev);
+void kt_renderer_destroy(kt_renderer* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KERRTRACE_H */

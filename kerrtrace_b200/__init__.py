@@ -1,0 +1,349 @@
+"""kerrtrace_b200 — B200-native KerrTrace geodesic hot path (Python host binding).
+
+The product is the C-ABI library ``libkerrtrace.so`` (include/kerrtrace.h) built from
+``csrc/`` for sm_100a.  This module binds it with ctypes and mirrors the reference's renderer
+interface (src/renderer/mod.rs: ``CudaRenderer::{new, submit_render, ready_frame,
+finish_frame}``) plus the kernel-level entry points that replace the reference's three launches.
+Nothing here computes on the CPU: if the library is missing the import of the binding fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libkerrtrace.so"
+
+KT_OK = 0
+KT_ERR_INVALID_ARG = 1
+KT_ERR_CUDA = 2
+KT_ERR_LUT_OVERFLOW = 3
+KT_ERR_NOT_READY = 4
+KT_ERR_QUEUE_ORDER = 5
+KT_ERR_NO_DEVICE = 6
+KT_ERR_UNSUPPORTED = 7
+KT_ERR_TIMEOUT = 8
+
+MODE_REF, MODE_SPEC = 0, 1
+PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
+SCHED_PLAIN, SCHED_WAVEFRONT = 0, 1
+
+
+class KtConfig(C.Structure):
+    """Mirror of ``kt_config`` (the reference's config.yaml fields, src/main.rs:15-122)."""
+
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32),
+        ("block_dim", C.c_uint32 * 2),
+        ("bloom_enabled", C.c_int32), ("bloom_intensity", C.c_float), ("bloom_radius", C.c_float),
+        ("lut_size", C.c_uint32), ("lut_max_temp", C.c_float),
+        ("wavelength_start", C.c_float), ("wavelength_end", C.c_float), ("wavelength_step", C.c_float),
+        ("use_fast_math", C.c_int32),
+        ("spp", C.c_uint32), ("exposure_scale", C.c_float),
+        ("sky_grid_divisions", C.c_uint32), ("sky_line_thickness", C.c_float), ("sky_intensity", C.c_float),
+        ("spin", C.c_float), ("mass", C.c_float),
+        ("disk_outer_radius", C.c_float), ("disk_temperature_scale", C.c_float),
+        ("initial_step", C.c_float), ("tolerance", C.c_float),
+        ("max_steps", C.c_uint32), ("max_attempts", C.c_uint32),
+        ("transmittance_cutoff", C.c_float), ("horizon_epsilon", C.c_float), ("escape_radius", C.c_float),
+        ("noise_enabled", C.c_int32), ("noise_scale", C.c_float), ("noise_strength", C.c_float),
+        ("noise_winding", C.c_float), ("noise_detail", C.c_uint32),
+        ("mode", C.c_int32), ("precision", C.c_int32), ("noise_seed", C.c_uint32),
+        ("noise_phase", C.c_float), ("bloom_threshold", C.c_float), ("photon_zone_factor", C.c_float),
+    ]
+
+    def copy(self) -> "KtConfig":
+        c = KtConfig()
+        C.memmove(C.byref(c), C.byref(self), C.sizeof(KtConfig))
+        return c
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if name == "block_dim" else v
+        return out
+
+
+class KtKerrParams(C.Structure):
+    """Mirror of ``kt_kerr_params`` / the reference's KerrParams (cuda/kerr_math.cuh:3-9)."""
+
+    _fields_ = [(n, C.c_float) for n in ("a", "m", "aa", "inv_m", "a_norm", "rh", "disk_inner",
+                                         "inv_w_2", "inv_h_2", "aspect_ratio", "disk_noise_scale",
+                                         "disk_noise_strength", "disk_noise_winding")] + [
+        ("disk_noise_enabled", C.c_int32), ("disk_noise_detail", C.c_int32)]
+
+
+class KtCamera(C.Structure):
+    _fields_ = [("cam_pos", C.c_float * 3), ("fwd", C.c_float * 3), ("rgt", C.c_float * 3),
+                ("up", C.c_float * 3), ("fov_scale", C.c_float)]
+
+
+class KtTraceStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("rays", "steps", "attempts", "rhs_evals", "frozen_rays", "fp64_steps")]
+
+
+class KtError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"kerrtrace status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+# (name, restype, argtypes) of every exported entry point of include/kerrtrace.h
+SIGNATURES = [
+    ("kt_status_str", C.c_char_p, [C.c_int]),
+    ("kt_last_error", C.c_char_p, []),
+    ("kt_abi_version", C.c_int, []),
+    ("kt_config_default", C.c_int, [C.POINTER(KtConfig)]),
+    ("kt_build_kerr_params", C.c_int, [C.POINTER(KtConfig), C.POINTER(KtKerrParams)]),
+    ("kt_calc_isco", C.c_float, [C.c_float, C.c_int, C.c_float]),
+    ("kt_generate_blackbody_lut", C.c_int, [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]),
+    ("kt_generate_disk_lut", C.c_int, [C.POINTER(KtKerrParams), C.c_float, C.c_uint32, C.c_void_p]),
+    ("kt_build_defines", C.c_int, [C.POINTER(KtConfig), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("kt_validate_bloom", C.c_int, [C.POINTER(KtConfig), C.POINTER(C.c_int32), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
+    ("kt_camera_basis", C.c_int, [C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                  C.POINTER(C.c_float)]),
+    ("kt_fov_scale", C.c_float, [C.c_float]),
+    ("kt_context_create", C.c_int, [C.POINTER(KtConfig), C.c_int, C.POINTER(C.c_void_p)]),
+    ("kt_context_create_with_luts", C.c_int, [C.POINTER(KtConfig), C.c_int, C.c_void_p, C.c_void_p, C.c_uint32,
+                                              C.POINTER(C.c_void_p)]),
+    ("kt_context_destroy", None, [C.c_void_p]),
+    ("kt_context_params", C.c_int, [C.c_void_p, C.POINTER(KtKerrParams)]),
+    ("kt_trace", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p]),
+    ("kt_trace_counted", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p,
+                                   C.POINTER(KtTraceStats)]),
+    ("kt_bloom_horizontal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_post_process", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_post_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_renderer_new", C.c_int, [C.POINTER(KtConfig), C.c_int, C.POINTER(C.c_void_p)]),
+    ("kt_renderer_submit_render", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                            C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
+                                            C.POINTER(C.c_int32)]),
+    ("kt_renderer_ready_frame", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.POINTER(C.c_uint32)),
+                                          C.POINTER(C.c_float)]),
+    ("kt_renderer_finish_frame", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("kt_renderer_wait", C.c_int, [C.c_void_p]),
+    ("kt_renderer_set_schedule", C.c_int, [C.c_void_p, C.c_int32]),
+    ("kt_renderer_frame_hdr", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("kt_renderer_destroy", None, [C.c_void_p]),
+]
+
+
+def lib() -> C.CDLL:
+    """Loads the in-tree C-ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m kerrtrace_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != KT_OK:
+        msg = lib().kt_last_error().decode() or lib().kt_status_str(status).decode()
+        raise KtError(status, msg)
+
+
+# ---- host precompute ----------------------------------------------------------------------
+
+def config_default() -> KtConfig:
+    c = KtConfig()
+    check(lib().kt_config_default(C.byref(c)))
+    return c
+
+
+def build_kerr_params(cfg: KtConfig) -> KtKerrParams:
+    p = KtKerrParams()
+    check(lib().kt_build_kerr_params(C.byref(cfg), C.byref(p)))
+    return p
+
+
+def generate_blackbody_lut(size, max_temp, wl_start, wl_end, wl_step):
+    import numpy as np
+    out = np.zeros((size, 4), dtype=np.float32)
+    check(lib().kt_generate_blackbody_lut(size, max_temp, wl_start, wl_end, wl_step, out.ctypes.data))
+    return out
+
+
+def generate_disk_lut(params: KtKerrParams, disk_outer: float, size: int):
+    import numpy as np
+    out = np.zeros(size, dtype=np.float32)
+    check(lib().kt_generate_disk_lut(C.byref(params), disk_outer, size, out.ctypes.data))
+    return out
+
+
+def build_defines(cfg: KtConfig) -> str:
+    n = C.c_size_t(0)
+    check(lib().kt_build_defines(C.byref(cfg), None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib().kt_build_defines(C.byref(cfg), buf, n.value + 1, C.byref(n)))
+    return buf.value.decode()
+
+
+def camera_basis(yaw_deg: float, pitch_deg: float):
+    """calculate_camera_basis (src/math.rs:3-14): (forward, right, up) with world-up +y."""
+    f = (C.c_float * 3)()
+    r = (C.c_float * 3)()
+    u = (C.c_float * 3)()
+    check(lib().kt_camera_basis(yaw_deg, pitch_deg, f, r, u))
+    return list(f), list(r), list(u)
+
+
+def make_camera(pos, yaw_deg: float, pitch_deg: float, fov_deg: float) -> KtCamera:
+    """Camera of submit_render from a position, yaw/pitch and vertical FOV (src/app.rs:158-170)."""
+    f, r, u = camera_basis(yaw_deg, pitch_deg)
+    cam = KtCamera()
+    for i in range(3):
+        cam.cam_pos[i] = pos[i]
+        cam.fwd[i] = f[i]
+        cam.rgt[i] = r[i]
+        cam.up[i] = u[i]
+    cam.fov_scale = lib().kt_fov_scale(fov_deg)
+    return cam
+
+
+def orbit_camera(r_obs: float, incl_deg: float, fov_deg: float, azimuth_deg: float = 0.0) -> KtCamera:
+    """Observer at Kerr-Schild radius r_obs, inclination from the spin axis (+y), looking at the
+    hole.  Azimuth 0 puts the camera in the x-y plane; yaw/pitch follow src/math.rs:3-14."""
+    i = math.radians(incl_deg)
+    az = math.radians(azimuth_deg)
+    pos = (r_obs * math.sin(i) * math.cos(az), r_obs * math.cos(i), r_obs * math.sin(i) * math.sin(az))
+    d = [-p / r_obs for p in pos]
+    pitch = math.degrees(math.asin(max(-1.0, min(1.0, d[1]))))
+    yaw = math.degrees(math.atan2(d[0], -d[2]))
+    return make_camera(pos, yaw, pitch, fov_deg)
+
+
+# ---- device objects -----------------------------------------------------------------------
+
+class Context:
+    """Device context: LUT textures + scene constants (replaces the reference's NVRTC module,
+    `c_params` upload and texture creation, src/renderer/init.rs:74-140)."""
+
+    def __init__(self, cfg: KtConfig, device: int = 0, luts=None):
+        self.cfg = cfg.copy()
+        h = C.c_void_p()
+        if luts is None:
+            check(lib().kt_context_create(C.byref(self.cfg), device, C.byref(h)))
+        else:
+            import numpy as np
+            bb = np.ascontiguousarray(luts[0], dtype=np.float32)
+            dk = np.ascontiguousarray(luts[1], dtype=np.float32)
+            check(lib().kt_context_create_with_luts(C.byref(self.cfg), device, bb.ctypes.data, dk.ctypes.data,
+                                                    dk.shape[0], C.byref(h)))
+        self.handle = h
+
+    def params(self) -> KtKerrParams:
+        p = KtKerrParams()
+        check(lib().kt_context_params(self.handle, C.byref(p)))
+        return p
+
+    def trace(self, cam: KtCamera, hdr_ptr: int, err_ptr: int, stream: int = 0, schedule: int = SCHED_WAVEFRONT):
+        check(lib().kt_trace(self.handle, C.c_void_p(stream), C.byref(cam), schedule, C.c_void_p(hdr_ptr),
+                             C.c_void_p(err_ptr)))
+
+    def trace_counted(self, cam: KtCamera, hdr_ptr: int, err_ptr: int, stream: int = 0,
+                      schedule: int = SCHED_WAVEFRONT) -> KtTraceStats:
+        st = KtTraceStats()
+        check(lib().kt_trace_counted(self.handle, C.c_void_p(stream), C.byref(cam), schedule, C.c_void_p(hdr_ptr),
+                                     C.c_void_p(err_ptr), C.byref(st)))
+        return st
+
+    def bloom_horizontal(self, hdr_ptr: int, bloom_ptr: int, stream: int = 0):
+        check(lib().kt_bloom_horizontal(self.handle, C.c_void_p(stream), C.c_void_p(hdr_ptr), C.c_void_p(bloom_ptr)))
+
+    def post_process(self, hdr_ptr: int, bloom_ptr: int, image_ptr: int, stream: int = 0):
+        check(lib().kt_post_process(self.handle, C.c_void_p(stream), C.c_void_p(hdr_ptr), C.c_void_p(bloom_ptr),
+                                    C.c_void_p(image_ptr)))
+
+    def post_fused(self, hdr_ptr: int, image_ptr: int, stream: int = 0):
+        check(lib().kt_post_fused(self.handle, C.c_void_p(stream), C.c_void_p(hdr_ptr), C.c_void_p(image_ptr)))
+
+    def close(self):
+        if self.handle:
+            lib().kt_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LutOverflow(KtError):
+    def __init__(self, temp: float, message: str):
+        super().__init__(KT_ERR_LUT_OVERFLOW, message)
+        self.temp = temp
+
+
+class Renderer:
+    """Mirror of the reference's CudaRenderer (src/renderer/mod.rs:469-687)."""
+
+    def __init__(self, cfg: KtConfig, device: int = 0):
+        self.cfg = cfg.copy()
+        h = C.c_void_p()
+        check(lib().kt_renderer_new(C.byref(self.cfg), device, C.byref(h)))
+        self.handle = h
+
+    def set_schedule(self, schedule: int):
+        check(lib().kt_renderer_set_schedule(self.handle, schedule))
+
+    def submit_render(self, cam_pos, fwd, rgt, up, fov_scale: float) -> bool:
+        arr = lambda v: (C.c_float * 3)(*v)  # noqa: E731
+        sub = C.c_int32(0)
+        check(lib().kt_renderer_submit_render(self.handle, arr(cam_pos), arr(fwd), arr(rgt), arr(up), fov_scale,
+                                              C.byref(sub)))
+        return bool(sub.value)
+
+    def ready_frame(self):
+        """Returns (index, numpy u32 view of the frame) or None when no frame is complete."""
+        import numpy as np
+        idx = C.c_uint32(0)
+        data = C.POINTER(C.c_uint32)()
+        temp = C.c_float(0.0)
+        st = lib().kt_renderer_ready_frame(self.handle, C.byref(idx), C.byref(data), C.byref(temp))
+        if st == KT_ERR_NOT_READY:
+            return None
+        if st == KT_ERR_LUT_OVERFLOW:
+            raise LutOverflow(temp.value, lib().kt_last_error().decode())
+        check(st)
+        n = self.cfg.width * self.cfg.height
+        view = np.ctypeslib.as_array(data, shape=(n,))
+        return idx.value, view
+
+    def finish_frame(self, index: int):
+        check(lib().kt_renderer_finish_frame(self.handle, index))
+
+    def wait(self):
+        check(lib().kt_renderer_wait(self.handle))
+
+    def frame_hdr_ptr(self, index: int) -> int:
+        p = C.c_void_p()
+        check(lib().kt_renderer_frame_hdr(self.handle, index, C.byref(p)))
+        return p.value
+
+    def close(self):
+        if self.handle:
+            lib().kt_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = [n for n in dir() if not n.startswith("_")]

@@ -1,0 +1,360 @@
+// kt_device.cuh — device-side geodesic core of the KerrTrace hot path (sm_100a).
+//
+// Restates, in this project's own structure, the per-ray algorithm of the reference:
+//   cuda/kerr_math.cuh   (Kerr-Schild radius, Hamiltonian RHS, DP dense output, PCG, FBM, sky)
+//   cuda/kerr_trace.cuh  (null initialisation, DP5(4) FSAL stepper, crossing, shading)
+//   cuda/kernel.cu:1-16  (LUT fetch with overflow flag)
+// The arithmetic of each formula is kept in the reference's order (same products, same
+// fused multiply-adds, same fast-math intrinsics) so that the FP32 path reproduces the
+// reference kernel's results; the scheduling around it (attempt-granular state machine,
+// persistent refill, retirement of NaN-frozen rays) is this project's.
+//
+// Everything is templated on the integration type R (float for the reference arithmetic,
+// double for the FP64 path); the mixed path uses float RHS with a double state update.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kt_types.h"
+
+namespace ktd {
+
+// ----------------------------------------------------------------------------------------
+// Arithmetic policies.  Ops<float> uses the intrinsics the reference calls (it is built with
+// use_fast_math, config.yaml:39); Ops<double> their IEEE double counterparts.
+// ----------------------------------------------------------------------------------------
+template <class R> struct Ops;
+template <> struct Ops<float> {
+    static __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float sqrt_rn(float x) { return __fsqrt_rn(x); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
+    static __device__ __forceinline__ float powr(float a, float b) { return __powf(a, b); }
+    static __device__ __forceinline__ float maxr(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float minr(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float absr(float a) { return fabsf(a); }
+    static __device__ __forceinline__ float expr(float a) { return __expf(a); }
+    static __device__ __forceinline__ float atan2r(float y, float x) { return atan2f(y, x); }
+    static __device__ __forceinline__ void sincosr(float a, float* s, float* c) { __sincosf(a, s, c); }
+    static __device__ __forceinline__ bool isnanr(float a) { return isnan(a); }
+    static __device__ __forceinline__ bool isfiniter(float a) { return isfinite(a); }
+};
+template <> struct Ops<double> {
+    static __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+    static __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double sqrt_rn(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
+    static __device__ __forceinline__ double powr(double a, double b) { return pow(a, b); }
+    static __device__ __forceinline__ double maxr(double a, double b) { return fmax(a, b); }
+    static __device__ __forceinline__ double minr(double a, double b) { return fmin(a, b); }
+    static __device__ __forceinline__ double absr(double a) { return fabs(a); }
+    static __device__ __forceinline__ double expr(double a) { return exp(a); }
+    static __device__ __forceinline__ double atan2r(double y, double x) { return atan2(y, x); }
+    static __device__ __forceinline__ void sincosr(double a, double* s, double* c) { sincos(a, s, c); }
+    static __device__ __forceinline__ bool isnanr(double a) { return isnan(a); }
+    static __device__ __forceinline__ bool isfiniter(double a) { return isfinite(a); }
+};
+
+// Literal of the integration type: the float spelling for float, the double one for double,
+// so that no constant is rounded twice.
+template <class R> __device__ __forceinline__ constexpr R lit(float f, double d);
+template <> __device__ __forceinline__ constexpr float lit<float>(float f, double) { return f; }
+template <> __device__ __forceinline__ constexpr double lit<double>(float, double d) { return d; }
+
+// Dormand-Prince 5(4) tableau (docs/dormand_prince_extended_tableau.md:1-12), evaluated in R
+// at compile time exactly as the reference's `static const float` initialisers
+// (cuda/kerr_trace.cuh:52-59).
+template <class R> struct DP {
+    static constexpr R a21 = R(1) / R(5);
+    static constexpr R a31 = R(3) / R(40), a32 = R(9) / R(40);
+    static constexpr R a41 = R(44) / R(45), a42 = R(-56) / R(15), a43 = R(32) / R(9);
+    static constexpr R a51 = R(19372) / R(6561), a52 = R(-25360) / R(2187),
+                       a53 = R(64448) / R(6561), a54 = R(-212) / R(729);
+    static constexpr R a61 = R(9017) / R(3168), a62 = R(-355) / R(33), a63 = R(46732) / R(5247),
+                       a64 = R(49) / R(176), a65 = R(-5103) / R(18656);
+    static constexpr R a71 = R(35) / R(384), a73 = R(500) / R(1113), a74 = R(125) / R(192),
+                       a75 = R(-2187) / R(6784), a76 = R(11) / R(84);
+    static constexpr R b1 = R(35) / R(384), b3 = R(500) / R(1113), b4 = R(125) / R(192),
+                       b5 = R(-2187) / R(6784), b6 = R(11) / R(84);
+    // embedded error weights b - b_hat
+    static constexpr R e1 = R(35) / R(384) - R(5179) / R(57600);
+    static constexpr R e3 = R(500) / R(1113) - R(7571) / R(16695);
+    static constexpr R e4 = R(125) / R(192) - R(393) / R(640);
+    static constexpr R e5 = R(-2187) / R(6784) + R(92097) / R(339200);
+    static constexpr R e6 = R(11) / R(84) - R(187) / R(2100);
+    static constexpr R e7 = R(-1) / R(40);
+    // Hairer continuous-extension weights (cuda/kerr_math.cuh:188-193)
+    static constexpr R d1 = R(-12715105075.0) / R(11282082432.0);
+    static constexpr R d3 = R(87487479700.0) / R(32700410799.0);
+    static constexpr R d4 = R(-10690763975.0) / R(1880347072.0);
+    static constexpr R d5 = R(701980252875.0) / R(199316789632.0);
+    static constexpr R d6 = R(-1453857185.0) / R(822651844.0);
+    static constexpr R d7 = R(69997945.0) / R(29380423.0);
+};
+
+// ---- PCG hash (cuda/kerr_math.cuh:26-36) ------------------------------------------------
+__device__ __forceinline__ uint32_t pcg_hash(uint64_t state) {
+    const uint64_t x = state * 6364136223846793005ULL + 1442695040888963407ULL;
+    const uint32_t xs = (uint32_t)(((x >> 18u) ^ x) >> 27u);
+    const uint32_t rot = (uint32_t)(x >> 59u);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+__device__ __forceinline__ float unit_float(uint64_t state) {
+    return (float)pcg_hash(state) * 2.3283064365386963e-10f;
+}
+
+// ---- Kerr-Schild radius with the spin along +y (cuda/kerr_math.cuh:50-59) ------------------
+template <class R>
+__device__ __forceinline__ R ks_radius(R x, R y, R z, R aa) {
+    using O = Ops<R>;
+    const R rho2 = O::fma(x, x, O::fma(y, y, z * z));
+    const R u = rho2 - aa;
+    const R s_sq = O::fma(u, u, R(4) * aa * y * y);
+    const R inv_s = O::rsq(s_sq);
+    const R s = s_sq * inv_s;
+    const R r2 = R(0.5) * (u + s);
+    return O::sqrt_rn(r2);
+}
+
+// ---- Hamiltonian right-hand side (cuda/kerr_math.cuh:82-156) -----------------------------
+// y = (x, y, z, p_x, p_y, p_z); p_t = pt is conserved.  With the Kerr-Schild potential
+// Hk = M r^3 / (r^4 + a^2 y^2) and null vector l, the RHS is
+//   dx/dl = p - 2 Hk (l.p - pt) l,   dp/dl = dHk/dx (l.p - pt)^2 + 2 Hk (l.p - pt) d(l.p)/dx.
+template <class R>
+__device__ __forceinline__ void hamilton_rhs(const R* __restrict__ st, R pt, R a, R aa, R M,
+                                             R* __restrict__ d) {
+    using O = Ops<R>;
+    const R x = st[0], y = st[1], z = st[2];
+    const R px = st[3], py = st[4], pz = st[5];
+    const R rho2 = O::fma(x, x, O::fma(y, y, z * z));
+    const R u = rho2 - aa;
+    const R s_sq = O::fma(u, u, R(4) * aa * y * y);
+    const R inv_s = O::rsq(s_sq);
+    const R r2 = R(0.5) * (u + s_sq * inv_s);
+    const R inv_r = O::rsq(r2);
+    const R r = r2 * inv_r;
+    // gradient of r via r^2
+    const R g2x = x * (R(1) + u * inv_s);
+    const R g2y = y * (R(1) + (u + R(4) * aa) * (R(0.5) * inv_s));
+    const R g2z = z * (R(1) + u * inv_s);
+    const R half_inv_r = R(0.5) * inv_r;
+    const R rx = g2x * half_inv_r;
+    const R ry = g2y * half_inv_r;
+    const R rz = g2z * half_inv_r;
+    // null vector l
+    const R den = r2 + aa;
+    const R inv_den = O::fdiv(R(1), den);
+    const R inv_den2 = inv_den * inv_den;
+    const R lx = (r * x - a * z) * inv_den;
+    const R ly = y * inv_r;
+    const R lz = (r * z + a * x) * inv_den;
+    // potential
+    const R r3 = r2 * r;
+    const R denH = O::fma(r2, r2, aa * y * y);
+    const R inv_denH = O::fdiv(R(1), denH);
+    const R Hk = M * r3 * inv_denH;
+    const R lp = O::fma(lx, px, O::fma(ly, py, O::fma(lz, pz, -pt)));
+    const R two_H_lp = R(2) * Hk * lp;
+    d[0] = px - two_H_lp * lx;
+    d[1] = py - two_H_lp * ly;
+    d[2] = pz - two_H_lp * lz;
+    // derivatives of l_x = Nx / D and l_z = Nz / D, D = r^2 + a^2
+    const R dDx = R(2) * r * rx;
+    const R dDy = R(2) * r * ry;
+    const R dDz = R(2) * r * rz;
+    const R Nx = r * x - a * z;
+    const R Nz = r * z + a * x;
+    const R dNx_x = rx * x + r;
+    const R dNx_y = ry * x;
+    const R dNx_z = rz * x - a;
+    const R dNz_x = rx * z + a;
+    const R dNz_y = ry * z;
+    const R dNz_z = rz * z + r;
+    const R dlx_x = (dNx_x * den - Nx * dDx) * inv_den2;
+    const R dlx_y = (dNx_y * den - Nx * dDy) * inv_den2;
+    const R dlx_z = (dNx_z * den - Nx * dDz) * inv_den2;
+    const R dlz_x = (dNz_x * den - Nz * dDx) * inv_den2;
+    const R dlz_y = (dNz_y * den - Nz * dDy) * inv_den2;
+    const R dlz_z = (dNz_z * den - Nz * dDz) * inv_den2;
+    // derivatives of l_y = y / r
+    const R inv_r2 = inv_r * inv_r;
+    const R dly_x = -y * rx * inv_r2;
+    const R dly_y = (r - y * ry) * inv_r2;
+    const R dly_z = -y * rz * inv_r2;
+    // derivatives of Hk
+    const R dHd_x = R(4) * r3 * rx;
+    const R dHd_y = O::fma(R(4) * r3, ry, R(2) * aa * y);
+    const R dHd_z = R(4) * r3 * rz;
+    const R inv_denH2 = inv_denH * inv_denH;
+    const R fH = M * inv_denH2;
+    const R dH_x = fH * (R(3) * r2 * rx * denH - r3 * dHd_x);
+    const R dH_y = fH * (R(3) * r2 * ry * denH - r3 * dHd_y);
+    const R dH_z = fH * (R(3) * r2 * rz * denH - r3 * dHd_z);
+    const R dlp_x = dlx_x * px + dly_x * py + dlz_x * pz;
+    const R dlp_y = dlx_y * px + dly_y * py + dlz_y * pz;
+    const R dlp_z = dlx_z * px + dly_z * py + dlz_z * pz;
+    const R lp2 = lp * lp;
+    d[3] = dH_x * lp2 + two_H_lp * dlp_x;
+    d[4] = dH_y * lp2 + two_H_lp * dlp_y;
+    d[5] = dH_z * lp2 + two_H_lp * dlp_z;
+}
+
+// ---- DOPRI5 continuous extension in the step fraction t (cuda/kerr_math.cuh:186-219) -------
+template <class R>
+__device__ __forceinline__ R dense_eval(R y0, R y1, R k1, R k3, R k4, R k5, R k6, R k7, R h, R t) {
+    using C = DP<R>;
+    const R q1 = y0;
+    const R q2 = y1 - y0;
+    const R q3 = y0 + h * k1 - y1;
+    const R q4 = R(2) * (y1 - y0) - h * (k1 + k7);
+    const R q5 = h * (C::d1 * k1 + C::d3 * k3 + C::d4 * k4 + C::d5 * k5 + C::d6 * k6 + C::d7 * k7);
+    const R t2 = t * t;
+    const R t3 = t2 * t;
+    const R t4 = t2 * t2;
+    return q1 + t * (q2 + q3) - t2 * (q3 - q4 - q5) - t3 * (q4 + R(2) * q5) + t4 * q5;
+}
+template <class R>
+__device__ __forceinline__ R dense_slope(R y0, R y1, R k1, R k3, R k4, R k5, R k6, R k7, R h, R t) {
+    using C = DP<R>;
+    const R q2 = y1 - y0;
+    const R q3 = y0 + h * k1 - y1;
+    const R q4 = R(2) * (y1 - y0) - h * (k1 + k7);
+    const R q5 = h * (C::d1 * k1 + C::d3 * k3 + C::d4 * k4 + C::d5 * k5 + C::d6 * k6 + C::d7 * k7);
+    const R t2 = t * t;
+    const R t3 = t2 * t;
+    return (q2 + q3) - R(2) * t * (q3 - q4 - q5) - R(3) * t2 * (q4 + R(2) * q5) + R(4) * t3 * q5;
+}
+
+// ---- gradient noise / FBM (cuda/kerr_math.cuh:172-179, 220-281) ----------------------------
+__device__ __forceinline__ float smooth5(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
+__device__ __forceinline__ float mixf(float a, float b, float t) { return fmaf(t, b - a, a); }
+__device__ __forceinline__ float2 lattice_gradient(int ix, int iy, unsigned seed) {
+    const uint64_t key = (((uint64_t)(uint32_t)ix) << 32) | (uint64_t)(uint32_t)iy;
+    const uint32_t hsh = pcg_hash(key ^ (uint64_t)seed);
+    constexpr float kAngle = 6.283185307f * 2.3283064365386963e-10f;
+    const float ang = (float)hsh * kAngle;
+    float sn, cs;
+    __sincosf(ang, &sn, &cs);
+    return make_float2(cs, sn);
+}
+__device__ __forceinline__ float gradient_noise2(float u, float v, unsigned seed) {
+    const int ix0 = __float2int_rd(u);
+    const int iy0 = __float2int_rd(v);
+    const int ix1 = ix0 + 1, iy1 = iy0 + 1;
+    const float fx = u - (float)ix0;
+    const float fy = v - (float)iy0;
+    const float2 g00 = lattice_gradient(ix0, iy0, seed);
+    const float2 g10 = lattice_gradient(ix1, iy0, seed);
+    const float2 g01 = lattice_gradient(ix0, iy1, seed);
+    const float2 g11 = lattice_gradient(ix1, iy1, seed);
+    const float n00 = g00.x * fx + g00.y * fy;
+    const float n10 = g10.x * (fx - 1.0f) + g10.y * fy;
+    const float n01 = g01.x * fx + g01.y * (fy - 1.0f);
+    const float n11 = g11.x * (fx - 1.0f) + g11.y * (fy - 1.0f);
+    const float uf = smooth5(fx);
+    const float vf = smooth5(fy);
+    const float m0 = mixf(n00, n10, uf);
+    const float m1 = mixf(n01, n11, uf);
+    return mixf(m0, m1, vf);
+}
+__device__ __forceinline__ float fbm2(float u, float v, int octaves, unsigned seed) {
+    if (octaves <= 0) return 0.5f;
+    float sum = 0.0f, amp = 1.0f, freq = 1.0f, amp_sum = 0.0f;
+    for (int o = 0; o < octaves; ++o) {
+        sum += gradient_noise2(u * freq, v * freq, seed) * amp;
+        amp_sum += amp;
+        amp *= 0.5f;
+        freq *= 2.0f;
+    }
+    float val = amp_sum > 0.0f ? (sum / amp_sum) : 0.0f;
+    return val * 0.5f + 0.5f;
+}
+
+// ---- procedural sky grid (cuda/kerr_math.cuh:157-171) -----------------------------------
+__device__ __forceinline__ float sky_value(float dx, float dy, float dz, float tau, const Scene& sc) {
+    const float lon = atan2f(dz, dx);
+    const float lat = asinf(dy);
+    const float spacing = sc.sky_spacing;
+    const float thick = sc.sky_thickness;
+    const float dlon = fmodf(fabsf(lon), spacing);
+    const float dlat = fmodf(fabsf(lat), spacing);
+    const bool on_line = (dlon < thick || dlon > (spacing - thick)) ||
+                         (dlat < thick || dlat > (spacing - thick)) ||
+                         (fabsf(lat) < thick * 3.0f);
+    return on_line ? (float)(sc.sky_intensity * (double)tau) : 0.0f;
+}
+
+// ---- LUT sampling ------------------------------------------------------------------------
+// Software form of a 1D linear, normalised, clamped texture fetch (full-precision weight).
+template <class R>
+__device__ __forceinline__ R lut_lerp1(const float* __restrict__ lut, int n, R u) {
+    const R x = u * R(n) - R(0.5);
+    const R fl = floor(x);
+    const R w = x - fl;
+    // clamp in floating point first so that NaN / huge coordinates cannot overflow the int
+    const R flc = fl < R(-1) ? R(-1) : (fl > R(n - 1) ? R(n - 1) : fl);
+    int i0 = fl == fl ? (int)flc : 0;
+    int i1 = i0 + 1;
+    i0 = i0 < 0 ? 0 : i0;
+    i1 = i1 > n - 1 ? n - 1 : i1;
+    const R v0 = (R)__ldg(lut + i0), v1 = (R)__ldg(lut + i1);
+    return v0 + w * (v1 - v0);
+}
+template <class R>
+__device__ __forceinline__ float4 lut_lerp4(const float4* __restrict__ lut, int n, R u) {
+    const R x = u * R(n) - R(0.5);
+    const R fl = floor(x);
+    const R w = x - fl;
+    // clamp in floating point first so that NaN / huge coordinates cannot overflow the int
+    const R flc = fl < R(-1) ? R(-1) : (fl > R(n - 1) ? R(n - 1) : fl);
+    int i0 = fl == fl ? (int)flc : 0;
+    int i1 = i0 + 1;
+    i0 = i0 < 0 ? 0 : i0;
+    i1 = i1 > n - 1 ? n - 1 : i1;
+    const float4 a = __ldg(lut + i0), b = __ldg(lut + i1);
+    return make_float4((float)(a.x + w * (b.x - a.x)), (float)(a.y + w * (b.y - a.y)),
+                       (float)(a.z + w * (b.z - a.z)), 0.0f);
+}
+
+// Blackbody colour of temperature T with the reference's overflow report
+// (cuda/kernel.cu:1-16): above lut_max_temp the first thread to notice records T.
+__device__ __forceinline__ float3 blackbody_rgb(float T, const Scene& sc, uint32_t* err) {
+    if (T > sc.lut_max_temp) {
+        if (atomicCAS(err, 0u, 1u) == 0u) err[1] = __float_as_uint(T);
+        return make_float3(0.0f, 0.0f, 0.0f);
+    }
+    const float tn = T / sc.lut_max_temp;
+    const float pos = tn * (float)(sc.lut_size - 1);
+    const float u = (pos + 0.5f) / (float)sc.lut_size;
+    float4 c;
+    if (sc.mode == 0) c = tex1D<float4>(sc.bb_tex, u);
+    else c = lut_lerp4<float>(sc.bb_lut, sc.lut_size, u);
+    return make_float3(c.x, c.y, c.z);
+}
+
+// ---- Boyer-Lindquist angles of a Kerr-Schild point (cuda/kerr_math.cuh:60-81) --------------
+template <class R>
+__device__ __forceinline__ void ks_to_bl(R x, R y, R z, R a, R aa, R& r, R& sin_th, R& cos_th,
+                                         R& phi) {
+    using O = Ops<R>;
+    const R rho2 = O::fma(x, x, O::fma(y, y, z * z));
+    const R u = rho2 - aa;
+    const R s_sq = O::fma(u, u, R(4) * aa * y * y);
+    const R inv_s = O::rsq(s_sq);
+    const R s = s_sq * inv_s;
+    const R r2 = R(0.5) * (u + s);
+    const R inv_r = O::rsq(r2);
+    r = r2 * inv_r;
+    cos_th = y * inv_r;
+    const R c2 = cos_th * cos_th;
+    const R s2 = R(1) - c2;
+    const R inv_sin = O::rsq(s2);
+    sin_th = s2 * inv_sin;
+    const R den = r2 + aa;
+    const R inv = inv_sin * O::fdiv(R(1), den);
+    const R cphi = (r * z + a * x) * inv;
+    const R sphi = (r * x - a * z) * inv;
+    phi = O::atan2r(sphi, cphi);
+}
+
+}  // namespace ktd

@@ -1,0 +1,925 @@
+// kt_host.cpp — C-ABI layer: host precompute, device context, CudaRenderer mirror.
+//
+// Host precompute restates the reference's Rust host in f32 arithmetic with the same libm
+// calls (Rust's f32::{cbrt, acos, cos, ln, exp, exp_m1} are the C library's cbrtf, acosf, cosf,
+// logf, expf, expm1f; mul_add is fmaf; this file is built with -ffp-contract=off so that no
+// other product is fused):
+//   build_kerr_params            src/renderer/utils.rs:53-113
+//   calc_isco                    src/renderer/utils.rs:11-20
+//   calc_novikov_thorne_factor   src/renderer/utils.rs:21-52
+//   generate_disk_temperature_lut src/renderer/utils.rs:172-201
+//   generate_blackbody_lut       src/renderer/blackbody.rs:6-124
+//   build_cuda_defines           src/renderer/utils.rs:115-163
+//   validate_bloom_settings      src/renderer/init.rs:43-73
+//   f32_from_f64                 src/math.rs:15-32 (shortest round-trip text, then parse)
+// Device context and renderer follow src/renderer/{texture,init,mod}.rs.
+#include <cuda_runtime.h>
+
+#include <charconv>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/kerrtrace.h"
+#include "kt_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+kt_status fail(kt_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+kt_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(KT_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+#define KT_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t e__ = (call);                        \
+        if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+    } while (0)
+
+// ---- numeric helpers ---------------------------------------------------------------------
+
+// src/math.rs:15-32: the f64 is printed with its shortest round-trip digits and that text is
+// parsed as f32.
+bool f32_from_f64(double v, float* out) {
+    if (!std::isfinite(v)) return false;
+    if (v < -(double)std::numeric_limits<float>::max() || v > (double)std::numeric_limits<float>::max()) return false;
+    char buf[64];
+    auto res = std::to_chars(buf, buf + sizeof buf - 1, v);
+    if (res.ec != std::errc()) return false;
+    *res.ptr = '\0';
+    const float f = std::strtof(buf, nullptr);
+    if (!std::isfinite(f)) return false;
+    *out = f;
+    return true;
+}
+
+// Value of the reference's `#define KEY {value:.10}` as the double literal the compiler sees.
+double define_value(float v) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "%.10f", (double)v);
+    return std::strtod(buf, nullptr);
+}
+float float_ceil(double d) {  // smallest float >= d
+    float f = (float)d;
+    if ((double)f < d) f = std::nextafterf(f, std::numeric_limits<float>::infinity());
+    return f;
+}
+float float_floor(double d) {  // largest float <= d
+    float f = (float)d;
+    if ((double)f > d) f = std::nextafterf(f, -std::numeric_limits<float>::infinity());
+    return f;
+}
+
+float isco_f32(float a_norm, bool prograde, float mass) {
+    const float aa = a_norm * a_norm;
+    const float z1 = fmaf(cbrtf(1.0f - aa), cbrtf(1.0f + a_norm) + cbrtf(1.0f - a_norm), 1.0f);
+    const float z2 = sqrtf(fmaf(3.0f, aa, z1 * z1));
+    const float sign = prograde ? -1.0f : 1.0f;
+    const float inside = (3.0f - z1) * fmaf(2.0f, z2, 3.0f + z1);
+    return mass * (3.0f + z2 + sign * sqrtf(fmaxf(inside, 0.0f)));
+}
+
+// Page-Thorne flux factor with the roots 2 cos(acos(-a)/3 - 2 pi k / 3) of x^3 - 3x + 2a = 0.
+float nt_factor_f32(float r, float a_norm, float r_isco, float inv_m) {
+    if (r <= r_isco) return 0.0f;
+    const float r_norm = r * inv_m;
+    const float r_isco_norm = r_isco * inv_m;
+    const float x = sqrtf(r_norm);
+    const float x_ms = sqrtf(r_isco_norm);
+    const float third = 1.0f / 3.0f;
+    const float angle_base = acosf(-a_norm) * third;
+    const float ang_step = 2.0943952f;
+    const float roots[3] = {2.0f * cosf(angle_base), 2.0f * cosf(angle_base - ang_step),
+                            2.0f * cosf(angle_base + ang_step)};
+    float sum_log = 0.0f;
+    for (int i = 0; i < 3; ++i) {
+        const float xi = roots[i];
+        const float den = xi * (xi - roots[(i + 1) % 3]) * (xi - roots[(i + 2) % 3]);
+        if (den <= 0.0f) continue;
+        const float coef = 3.0f * (xi - a_norm) * (xi - a_norm) / den;
+        const float val = (x - xi) / (x_ms - xi);
+        if (val > 0.0f) sum_log += coef * logf(val);
+    }
+    const float q = fmaf(1.5f * a_norm, -logf(x / x_ms), x - x_ms) - sum_log;
+    const float geo = r_norm * fmaf(2.0f, a_norm, fmaf(r_norm, x, -(3.0f * x)));
+    return fmaxf(q / geo, 0.0f);
+}
+
+float cmf_lobe(float x, float alpha, float mu, float s1, float s2) {
+    const float sigma = x < mu ? s1 : s2;
+    const float t = (x - mu) / sigma;
+    return alpha * expf(-0.5f * t * t);
+}
+
+bool finite_params(const kt_kerr_params& p) {
+    return std::isfinite(p.rh) && std::isfinite(p.disk_inner);
+}
+
+}  // namespace
+
+// =========================================================================================
+extern "C" {
+
+const char* kt_status_str(kt_status s) {
+    switch (s) {
+        case KT_OK: return "ok";
+        case KT_ERR_INVALID_ARG: return "invalid argument";
+        case KT_ERR_CUDA: return "CUDA error";
+        case KT_ERR_LUT_OVERFLOW: return "colour temperature above lut_max_temp";
+        case KT_ERR_NOT_READY: return "not ready";
+        case KT_ERR_QUEUE_ORDER: return "frame queue out of order";
+        case KT_ERR_NO_DEVICE: return "no CUDA device";
+        case KT_ERR_UNSUPPORTED: return "unsupported";
+        case KT_ERR_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+const char* kt_last_error(void) { return g_last_error.c_str(); }
+int kt_abi_version(void) { return KT_ABI_VERSION; }
+
+kt_status kt_config_default(kt_config* c) {
+    if (!c) return fail(KT_ERR_INVALID_ARG, "cfg is NULL");
+    std::memset(c, 0, sizeof *c);
+    c->width = 2100;
+    c->height = 900;
+    c->block_dim[0] = 16;
+    c->block_dim[1] = 16;
+    c->bloom_enabled = 1;
+    c->bloom_intensity = 0.5f;
+    c->bloom_radius = 48.0f;
+    c->lut_size = 4096;
+    c->lut_max_temp = 3e4f;
+    c->wavelength_start = 380.0f;
+    c->wavelength_end = 720.0f;
+    c->wavelength_step = 10.0f;
+    c->use_fast_math = 1;
+    c->spp = 4;
+    c->exposure_scale = 3e-3f;
+    c->sky_grid_divisions = 40;
+    c->sky_line_thickness = 5e-4f;
+    c->sky_intensity = 30.0f;
+    c->spin = -0.45f;
+    c->mass = 0.5f;
+    c->disk_outer_radius = 40.0f;
+    c->disk_temperature_scale = 3e4f;
+    c->initial_step = 1.0f;
+    c->tolerance = 1e-5f;
+    c->max_steps = 100;
+    c->max_attempts = 3;
+    c->transmittance_cutoff = 1e-2f;
+    c->horizon_epsilon = 5e-7f;
+    c->escape_radius = 80.0f;
+    c->noise_enabled = 1;
+    c->noise_scale = 0.1f;
+    c->noise_strength = 0.6f;
+    c->noise_winding = 50.0f;
+    c->noise_detail = 10;
+    c->mode = KT_MODE_REF;
+    c->precision = KT_PREC_FP32;
+    c->photon_zone_factor = 1.5f;
+    return KT_OK;
+}
+
+float kt_calc_isco(float a_norm, int prograde, float mass) { return isco_f32(a_norm, prograde != 0, mass); }
+
+kt_status kt_build_kerr_params(const kt_config* cfg, kt_kerr_params* out) {
+    if (!cfg || !out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (cfg->width == 0) return fail(KT_ERR_INVALID_ARG, "window width must not be 0");
+    if (cfg->height == 0) return fail(KT_ERR_INVALID_ARG, "window height must not be 0");
+    const float spin = cfg->spin, mass = cfg->mass;
+    if (!std::isfinite(spin)) return fail(KT_ERR_INVALID_ARG, "black hole spin is not finite: %g", spin);
+    if (!std::isfinite(mass)) return fail(KT_ERR_INVALID_ARG, "black hole mass is not finite: %g", mass);
+    if (mass == 0.0f) return fail(KT_ERR_INVALID_ARG, "black hole mass must not be 0");
+    kt_kerr_params p;
+    std::memset(&p, 0, sizeof p);
+    p.a = spin;
+    p.m = mass;
+    p.inv_m = 1.0f / mass;
+    p.aa = spin * spin;
+    p.a_norm = spin * p.inv_m;
+    p.rh = mass + sqrtf(fmaxf(fmaf(mass, mass, -p.aa), 0.0f));
+    p.disk_inner = isco_f32(p.a_norm, true, mass);
+    if (!finite_params(p)) return fail(KT_ERR_INVALID_ARG, "Kerr parameters are not finite");
+    if (!std::isfinite(cfg->noise_scale)) return fail(KT_ERR_INVALID_ARG, "disk noise scale is not finite");
+    if (!std::isfinite(cfg->noise_strength)) return fail(KT_ERR_INVALID_ARG, "disk noise strength is not finite");
+    if (!std::isfinite(cfg->noise_winding)) return fail(KT_ERR_INVALID_ARG, "disk noise winding is not finite");
+    if (cfg->noise_detail > (uint32_t)std::numeric_limits<int32_t>::max())
+        return fail(KT_ERR_INVALID_ARG, "disk noise detail out of i32 range: %u", cfg->noise_detail);
+    const double w = (double)cfg->width, h = (double)cfg->height;
+    if (!f32_from_f64(w / h, &p.aspect_ratio) || !f32_from_f64(2.0 / w, &p.inv_w_2) ||
+        !f32_from_f64(2.0 / h, &p.inv_h_2))
+        return fail(KT_ERR_INVALID_ARG, "window size conversion failed");
+    p.disk_noise_scale = cfg->noise_scale;
+    p.disk_noise_strength = cfg->noise_strength;
+    p.disk_noise_winding = cfg->noise_winding;
+    p.disk_noise_enabled = cfg->noise_enabled ? 1 : 0;
+    p.disk_noise_detail = (int32_t)cfg->noise_detail;
+    *out = p;
+    return KT_OK;
+}
+
+kt_status kt_generate_blackbody_lut(uint32_t size, float max_temp, float wl_start, float wl_end,
+                                    float wl_step, float* out) {
+    if (!out) return fail(KT_ERR_INVALID_ARG, "out is NULL");
+    if (size < 2) return fail(KT_ERR_INVALID_ARG, "blackbody LUT size must be at least 2");
+    if (!std::isfinite(wl_step) || wl_step <= 0.0f)
+        return fail(KT_ERR_INVALID_ARG, "wavelength step must be positive and finite");
+    std::vector<float> temps(size);
+    for (uint32_t i = 0; i < size; ++i) {
+        const double ratio = (double)i / (double)(size - 1);
+        if (!f32_from_f64(ratio * (double)max_temp, &temps[i]))
+            return fail(KT_ERR_INVALID_ARG, "temperature value conversion failed");
+    }
+    std::vector<float> lambdas;
+    for (float l = wl_start;;) {
+        if (l > wl_end) break;
+        lambdas.push_back(l);
+        l += wl_step;
+        if (lambdas.size() > (1u << 24)) return fail(KT_ERR_INVALID_ARG, "wavelength grid too large");
+    }
+    const size_t n = lambdas.size();
+    std::vector<float> xs(n), ys(n), zs(n);
+    for (size_t i = 0; i < n; ++i) {
+        const float l = lambdas[i];
+        xs[i] = cmf_lobe(l, 1.056f, 599.8f, 37.9f, 31.0f) + cmf_lobe(l, 0.362f, 442.0f, 16.0f, 26.7f) +
+                cmf_lobe(l, -0.065f, 501.1f, 20.4f, 26.2f);
+        ys[i] = cmf_lobe(l, 0.821f, 568.8f, 46.9f, 40.5f) + cmf_lobe(l, 0.286f, 530.9f, 16.3f, 31.1f);
+        zs[i] = cmf_lobe(l, 1.217f, 437.0f, 11.8f, 36.0f) + cmf_lobe(l, 0.681f, 459.0f, 26.2f, 13.8f);
+    }
+    const float c2 = 1.4388e7f;
+    for (uint32_t ti = 0; ti < size; ++ti) {
+        const float t = temps[ti];
+        float* row = out + 4 * (size_t)ti;
+        if (t == 0.0f) {
+            row[0] = row[1] = row[2] = row[3] = 0.0f;
+            continue;
+        }
+        float xsum = 0.0f, ysum = 0.0f, zsum = 0.0f;
+        for (size_t i = 0; i < n; ++i) {
+            float inten = 0.0f;
+            if (t > 0.0f) {
+                const float l = lambdas[i];
+                const float expo = c2 / (l * t);
+                if (!(expo > 80.0f)) {
+                    const float l2 = l * l;
+                    const float l5 = l * (l2 * l2);
+                    inten = ((1.0f / l5) / expm1f(expo)) * 1e15f;
+                }
+            }
+            xsum += inten * xs[i];
+            ysum += inten * ys[i];
+            zsum += inten * zs[i];
+        }
+        xsum *= wl_step;
+        ysum *= wl_step;
+        zsum *= wl_step;
+        row[0] = fmaf(3.240454f, xsum, fmaf(-1.5371385f, ysum, -0.4985314f * zsum));
+        row[1] = fmaf(-0.969266f, xsum, fmaf(1.8760108f, ysum, 0.041556f * zsum));
+        row[2] = fmaf(0.0556434f, xsum, fmaf(-0.2040259f, ysum, 1.0572252f * zsum));
+        row[3] = 0.0f;
+    }
+    return KT_OK;
+}
+
+kt_status kt_generate_disk_lut(const kt_kerr_params* p, float disk_outer, uint32_t size, float* out) {
+    if (!p || !out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (size < 2) return fail(KT_ERR_INVALID_ARG, "disk temperature LUT size must be at least 2");
+    if (!std::isfinite(disk_outer)) return fail(KT_ERR_INVALID_ARG, "disk outer radius is not finite");
+    if (!std::isfinite(p->disk_inner)) return fail(KT_ERR_INVALID_ARG, "disk inner radius is not finite");
+    if (disk_outer <= p->disk_inner)
+        return fail(KT_ERR_INVALID_ARG, "disk outer radius must exceed the inner radius: outer=%g, inner=%g",
+                    disk_outer, p->disk_inner);
+    const double inner = (double)p->disk_inner;
+    const double span = (double)(disk_outer - p->disk_inner);
+    for (uint32_t i = 0; i < size; ++i) {
+        const double ratio = (double)i / (double)(size - 1);
+        float r;
+        if (!f32_from_f64(std::fma(ratio, span, inner), &r)) return fail(KT_ERR_INVALID_ARG, "disk radius conversion failed");
+        const float f = nt_factor_f32(r, p->a_norm, p->disk_inner, p->inv_m);
+        if (!std::isfinite(f)) return fail(KT_ERR_INVALID_ARG, "disk flux factor is not finite");
+        const float v = sqrtf(sqrtf(f));
+        if (!std::isfinite(v)) return fail(KT_ERR_INVALID_ARG, "disk temperature factor is not finite");
+        out[i] = v;
+    }
+    return KT_OK;
+}
+
+kt_status kt_build_defines(const kt_config* cfg, char* buf, size_t cap, size_t* len) {
+    if (!cfg) return fail(KT_ERR_INVALID_ARG, "cfg is NULL");
+    std::string s;
+    char line[160];
+    const struct { const char* k; uint32_t v; } ints[] = {
+        {"CONFIG_SPP", cfg->spp},
+        {"CONFIG_SKY_GRID_DIVISIONS", cfg->sky_grid_divisions},
+        {"CONFIG_INTEGRATOR_MAX_STEPS", cfg->max_steps},
+        {"CONFIG_INTEGRATOR_MAX_ATTEMPTS", cfg->max_attempts},
+    };
+    for (auto& e : ints) {
+        snprintf(line, sizeof line, "#define %s %u\n", e.k, e.v);
+        s += line;
+    }
+    const struct { const char* k; float v; } floats[] = {
+        {"CONFIG_EXPOSURE_SCALE", cfg->exposure_scale},
+        {"CONFIG_SKY_LINE_THICKNESS", cfg->sky_line_thickness},
+        {"CONFIG_SKY_INTENSITY", cfg->sky_intensity},
+        {"CONFIG_DISK_OUTER_RADIUS", cfg->disk_outer_radius},
+        {"CONFIG_DISK_TEMPERATURE_SCALE", cfg->disk_temperature_scale},
+        {"CONFIG_INTEGRATOR_INITIAL_STEP", cfg->initial_step},
+        {"CONFIG_INTEGRATOR_TOLERANCE", cfg->tolerance},
+        {"CONFIG_TRANSMITTANCE_CUTOFF", cfg->transmittance_cutoff},
+        {"CONFIG_HORIZON_EPSILON", cfg->horizon_epsilon},
+        {"CONFIG_ESCAPE_RADIUS", cfg->escape_radius},
+        {"CONFIG_BLACKBODY_WAVELENGTH_STEP", cfg->wavelength_step},
+    };
+    for (auto& e : floats) {
+        snprintf(line, sizeof line, "#define %s %.10f\n", e.k, (double)e.v);
+        s += line;
+    }
+    if (len) *len = s.size();
+    if (buf) {
+        if (cap < s.size() + 1) return fail(KT_ERR_INVALID_ARG, "buffer too small (%zu < %zu)", cap, s.size() + 1);
+        std::memcpy(buf, s.c_str(), s.size() + 1);
+    }
+    return KT_OK;
+}
+
+static void vnormalize(float v[3]) {
+    const float len = sqrtf((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+    const float inv = 1.0f / len;
+    v[0] *= inv;
+    v[1] *= inv;
+    v[2] *= inv;
+}
+static void vcross(const float a[3], const float b[3], float o[3]) {
+    o[0] = a[1] * b[2] - b[1] * a[2];
+    o[1] = a[2] * b[0] - b[2] * a[0];
+    o[2] = a[0] * b[1] - b[0] * a[1];
+}
+static const float kRadsPerDeg = 3.14159265358979323846f / 180.0f;  // f32::to_radians
+
+kt_status kt_camera_basis(float yaw_deg, float pitch_deg, float fwd[3], float rgt[3], float up[3]) {
+    if (!fwd || !rgt || !up) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    const float yaw = yaw_deg * kRadsPerDeg, pitch = pitch_deg * kRadsPerDeg;
+    float f[3] = {sinf(yaw) * cosf(pitch), sinf(pitch), -cosf(yaw) * cosf(pitch)};
+    vnormalize(f);
+    const float world_up[3] = {0.0f, 1.0f, 0.0f};
+    float r[3], u[3];
+    vcross(f, world_up, r);
+    vnormalize(r);
+    vcross(r, f, u);
+    vnormalize(u);
+    for (int i = 0; i < 3; ++i) {
+        fwd[i] = f[i];
+        rgt[i] = r[i];
+        up[i] = u[i];
+    }
+    return KT_OK;
+}
+
+float kt_fov_scale(float fov_deg) { return tanf((fov_deg * kRadsPerDeg) / 2.0f); }
+
+kt_status kt_validate_bloom(const kt_config* cfg, int32_t* enabled, float* intensity, float* radius,
+                            int32_t* radius_int) {
+    if (!cfg) return fail(KT_ERR_INVALID_ARG, "cfg is NULL");
+    const float inten = cfg->bloom_intensity;
+    if (!std::isfinite(inten) || inten < 0.0f) return fail(KT_ERR_INVALID_ARG, "invalid bloom intensity: %g", inten);
+    const float rad = cfg->bloom_radius;
+    if (!std::isfinite(rad) || rad < 0.0f) return fail(KT_ERR_INVALID_ARG, "invalid bloom radius: %g", rad);
+    const double max_r = (double)std::numeric_limits<int32_t>::max();
+    if ((double)rad > max_r) return fail(KT_ERR_INVALID_ARG, "bloom radius too large: %g", rad);
+    int32_t ri = 0;
+    if (rad > 0.0f) {
+        const float c = ceilf(rad);
+        if ((double)c > max_r) return fail(KT_ERR_INVALID_ARG, "bloom radius too large: %g", rad);
+        ri = (int32_t)c;
+    }
+    if (enabled) *enabled = cfg->bloom_enabled ? 1 : 0;
+    if (intensity) *intensity = inten;
+    if (radius) *radius = rad;
+    if (radius_int) *radius_int = ri;
+    return KT_OK;
+}
+
+}  // extern "C"
+
+// =========================================================================================
+// Device context
+// =========================================================================================
+struct kt_context {
+    int device = 0;
+    kt_config cfg{};
+    kt_kerr_params params{};
+    ktd::Scene scene{};
+    ktd::PostParams post{};
+    cudaArray_t bb_array = nullptr, disk_array = nullptr;
+    cudaTextureObject_t bb_tex = 0, disk_tex = 0;
+    float4* bb_lut_dev = nullptr;
+    float* disk_lut_dev = nullptr;
+    unsigned* queue = nullptr;              // wavefront work counter (1 word)
+    unsigned long long* counters = nullptr; // 6 x u64 for the counting launches
+    int block_x = 16, block_y = 16;
+};
+
+namespace {
+
+void destroy_ctx(kt_context* c) {
+    if (!c) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(c->device);
+    if (c->bb_tex) cudaDestroyTextureObject(c->bb_tex);
+    if (c->disk_tex) cudaDestroyTextureObject(c->disk_tex);
+    if (c->bb_array) cudaFreeArray(c->bb_array);
+    if (c->disk_array) cudaFreeArray(c->disk_array);
+    cudaFree(c->bb_lut_dev);
+    cudaFree(c->disk_lut_dev);
+    cudaFree(c->queue);
+    cudaFree(c->counters);
+    cudaSetDevice(prev);
+    delete c;
+}
+
+// 1D cudaArray + texture object with the reference's sampler (texture.rs:86-202): float
+// channels, linear filtering, normalised coordinates, clamp addressing.  The blackbody LUT is
+// allocated with height 1, the disk LUT with height 0, as in texture.rs:37-67.
+kt_status make_lut_texture(const float* host, uint32_t n, int channels, size_t height,
+                           cudaArray_t* arr, cudaTextureObject_t* tex) {
+    const cudaChannelFormatDesc desc =
+        channels == 4 ? cudaCreateChannelDesc(32, 32, 32, 32, cudaChannelFormatKindFloat)
+                      : cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+    KT_CUDA(cudaMallocArray(arr, &desc, n, height, cudaArrayDefault), "cudaMallocArray");
+    const size_t row_bytes = (size_t)n * channels * sizeof(float);
+    KT_CUDA(cudaMemcpy2DToArray(*arr, 0, 0, host, row_bytes, row_bytes, 1, cudaMemcpyHostToDevice),
+            "copy LUT to CUDA array");
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof rd);
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = *arr;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof td);
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    KT_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+    return KT_OK;
+}
+
+kt_status fill_scene(kt_context* c) {
+    const kt_config& cfg = c->cfg;
+    const kt_kerr_params& p = c->params;
+    ktd::Scene& s = c->scene;
+    std::memset(&s, 0, sizeof s);
+    s.a = p.a; s.M = p.m; s.aa = p.aa; s.inv_M = p.inv_m; s.a_norm = p.a_norm; s.rh = p.rh;
+    s.disk_inner = p.disk_inner;
+    s.disk_outer = cfg.disk_outer_radius;
+    s.inv_w_2 = p.inv_w_2; s.inv_h_2 = p.inv_h_2; s.aspect = p.aspect_ratio;
+    s.noise_scale = p.disk_noise_scale; s.noise_strength = p.disk_noise_strength;
+    s.noise_winding = p.disk_noise_winding; s.noise_enabled = p.disk_noise_enabled;
+    s.noise_detail = p.disk_noise_detail;
+    const uint32_t imax = (uint32_t)std::numeric_limits<int32_t>::max();
+    if (cfg.spp > imax || cfg.max_steps > imax || cfg.max_attempts > imax || cfg.sky_grid_divisions > imax)
+        return fail(KT_ERR_INVALID_ARG, "integer knob out of i32 range");
+    if (cfg.max_attempts == 0) return fail(KT_ERR_INVALID_ARG, "max_attempts must be at least 1");
+    s.spp = (int)cfg.spp;
+    s.max_steps = (int)cfg.max_steps;
+    s.max_attempts = (int)cfg.max_attempts;
+    s.sky_div = (int)cfg.sky_grid_divisions;
+    s.sky_spacing = 3.14159265f / (float)cfg.sky_grid_divisions;
+    const double d_exposure = define_value(cfg.exposure_scale);
+    const double d_thick = define_value(cfg.sky_line_thickness);
+    const double d_sky = define_value(cfg.sky_intensity);
+    const double d_temp = define_value(cfg.disk_temperature_scale);
+    const double d_h0 = define_value(cfg.initial_step);
+    const double d_tol = define_value(cfg.tolerance);
+    const double d_cut = define_value(cfg.transmittance_cutoff);
+    const double d_heps = define_value(cfg.horizon_epsilon);
+    const double d_esc = define_value(cfg.escape_radius);
+    const double d_wl = define_value(cfg.wavelength_step);
+    s.h0 = (float)d_h0;
+    s.base_tol = (float)d_tol;
+    s.sky_thickness = (float)d_thick;
+    s.horizon_lt = float_ceil((double)p.rh + d_heps);
+    s.escape_gt = float_floor(d_esc);
+    s.cutoff_gt = float_floor(d_cut);
+    const float inv_spp = 1.0f / (float)cfg.spp;
+    s.final_scale = (float)(d_exposure * (double)inv_spp);
+    s.temp_scale = d_temp;
+    s.wl_step = d_wl;
+    s.sky_intensity = d_sky;
+    s.a_d = (double)p.a;
+    s.aa_d = s.a_d * s.a_d;
+    s.M_d = (double)p.m;
+    const double rh_d = s.M_d + std::sqrt(std::fmax(s.M_d * s.M_d - s.aa_d, 0.0));
+    s.horizon_d = (double)p.rh + d_heps;  // the reference adds the define to the f32 rh
+    (void)rh_d;
+    s.escape_d = d_esc;
+    s.cutoff_d = d_cut;
+    s.h0_d = d_h0;
+    s.base_tol_d = d_tol;
+    s.bb_tex = c->bb_tex;
+    s.disk_tex = c->disk_tex;
+    s.bb_lut = c->bb_lut_dev;
+    s.disk_lut = c->disk_lut_dev;
+    s.lut_size = (int)cfg.lut_size;
+    s.lut_max_temp = cfg.lut_max_temp;
+    s.mode = cfg.mode;
+    s.precision = cfg.precision;
+    s.noise_seed = cfg.noise_seed;
+    s.noise_phase = cfg.noise_phase;
+    const float zf = cfg.photon_zone_factor > 0.0f ? cfg.photon_zone_factor : 1.5f;
+    // prograde equatorial photon orbit r_ph = 2M (1 + cos(2/3 acos(-|a|/M)))
+    const double an = std::fabs((double)p.a_norm);
+    const double rph = 2.0 * s.M_d * (1.0 + std::cos(2.0 / 3.0 * std::acos(-std::fmin(an, 1.0))));
+    s.zone_r = (float)(zf * std::fmax(rph, 3.0 * s.M_d));
+    s.spec_tol_floor = 1.0f;
+    s.width = (int)cfg.width;
+    s.height = (int)cfg.height;
+    return KT_OK;
+}
+
+kt_status fill_post(kt_context* c) {
+    int32_t en = 0, ri = 0;
+    float inten = 0.0f, rad = 0.0f;
+    kt_status st = kt_validate_bloom(&c->cfg, &en, &inten, &rad, &ri);
+    if (st != KT_OK) return st;
+    ktd::PostParams& pp = c->post;
+    pp.width = (int)c->cfg.width;
+    pp.height = (int)c->cfg.height;
+    pp.radius = ri;
+    pp.sigma = rad / 3.0f;
+    pp.intensity = inten;
+    pp.active = (en && ri > 0 && inten > 0.0f) ? 1 : 0;
+    pp.mode = c->cfg.mode;
+    pp.threshold = c->cfg.bloom_threshold;
+    return KT_OK;
+}
+
+kt_status validate_cfg(const kt_config* cfg) {
+    if (!cfg) return fail(KT_ERR_INVALID_ARG, "cfg is NULL");
+    if (!cfg->use_fast_math) return fail(KT_ERR_UNSUPPORTED, "the kernels are built with use_fast_math; use_fast_math=false is not available");
+    if (cfg->mode != KT_MODE_REF && cfg->mode != KT_MODE_SPEC) return fail(KT_ERR_INVALID_ARG, "unknown mode %d", cfg->mode);
+    if (cfg->precision < KT_PREC_FP32 || cfg->precision > KT_PREC_FP64) return fail(KT_ERR_INVALID_ARG, "unknown precision %d", cfg->precision);
+    if (cfg->mode == KT_MODE_REF && cfg->precision != KT_PREC_FP32)
+        return fail(KT_ERR_INVALID_ARG, "reference mode runs the reference's FP32 arithmetic; use KT_MODE_SPEC for mixed/FP64");
+    if (cfg->width > 32768 || cfg->height > 32768 || (uint64_t)cfg->width * cfg->height > (1ull << 31))
+        return fail(KT_ERR_INVALID_ARG, "image too large: %ux%u", cfg->width, cfg->height);
+    const uint64_t bt = (uint64_t)cfg->block_dim[0] * cfg->block_dim[1];
+    if (cfg->block_dim[0] == 0 || cfg->block_dim[1] == 0 || bt > 1024)
+        return fail(KT_ERR_INVALID_ARG, "block_dim %ux%u must be non-zero with at most 1024 threads",
+                    cfg->block_dim[0], cfg->block_dim[1]);
+    if (cfg->lut_size < 2) return fail(KT_ERR_INVALID_ARG, "lut_size must be at least 2");
+    if (!std::isfinite(cfg->lut_max_temp)) return fail(KT_ERR_INVALID_ARG, "lut_max_temp is not finite");
+    return KT_OK;
+}
+
+kt_status create_impl(const kt_config* cfg, int device, const float* bb_in, const float* disk_in,
+                      uint32_t lut_n, kt_context** out) {
+    if (!out) return fail(KT_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    kt_status st = validate_cfg(cfg);
+    if (st != KT_OK) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return fail(KT_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(KT_ERR_INVALID_ARG, "device %d out of range", device);
+    kt_context* c = new (std::nothrow) kt_context();
+    if (!c) return fail(KT_ERR_INVALID_ARG, "out of host memory");
+    c->device = device;
+    c->cfg = *cfg;
+    c->block_x = (int)cfg->block_dim[0];
+    c->block_y = (int)cfg->block_dim[1];
+    auto bail = [&](kt_status s) { destroy_ctx(c); return s; };
+    if ((st = kt_build_kerr_params(cfg, &c->params)) != KT_OK) return bail(st);
+    if ((st = fill_post(c)) != KT_OK) return bail(st);
+    const uint32_t n = cfg->lut_size;
+    std::vector<float> bb, disk;
+    if (bb_in) {
+        if (lut_n != n) return bail(fail(KT_ERR_INVALID_ARG, "LUT length %u does not match lut_size %u", lut_n, n));
+        bb.assign(bb_in, bb_in + 4 * (size_t)n);
+        disk.assign(disk_in, disk_in + n);
+    } else {
+        bb.resize(4 * (size_t)n);
+        disk.resize(n);
+        if ((st = kt_generate_blackbody_lut(n, cfg->lut_max_temp, cfg->wavelength_start, cfg->wavelength_end,
+                                            cfg->wavelength_step, bb.data())) != KT_OK)
+            return bail(st);
+        if ((st = kt_generate_disk_lut(&c->params, cfg->disk_outer_radius, n, disk.data())) != KT_OK) return bail(st);
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(KT_ERR_CUDA, "cudaSetDevice(%d) failed", device));
+    auto step = [&](kt_status s) { if (s != KT_OK) { cudaSetDevice(prev); destroy_ctx(c); } return s; };
+    if ((st = step(make_lut_texture(bb.data(), n, 4, 1, &c->bb_array, &c->bb_tex))) != KT_OK) return st;
+    if ((st = step(make_lut_texture(disk.data(), n, 1, 0, &c->disk_array, &c->disk_tex))) != KT_OK) return st;
+    cudaError_t e;
+    if ((e = cudaMalloc(&c->bb_lut_dev, bb.size() * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->disk_lut_dev, disk.size() * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->queue, 64)) != cudaSuccess ||
+        (e = cudaMalloc(&c->counters, 8 * sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMemcpy(c->bb_lut_dev, bb.data(), bb.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(c->disk_lut_dev, disk.data(), disk.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return step(cuda_fail(e, "context allocation"));
+    if ((st = step(fill_scene(c))) != KT_OK) return st;
+    cudaSetDevice(prev);
+    *out = c;
+    return KT_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev); else prev = -1;
+    }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+ktd::Camera to_camera(const kt_camera* cam) {
+    ktd::Camera c;
+    for (int i = 0; i < 3; ++i) {
+        c.pos[i] = cam->cam_pos[i];
+        c.fwd[i] = cam->fwd[i];
+        c.rgt[i] = cam->rgt[i];
+        c.up[i] = cam->up[i];
+    }
+    c.fov_scale = cam->fov_scale;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+kt_status kt_context_create(const kt_config* cfg, int device, kt_context** out) {
+    return create_impl(cfg, device, nullptr, nullptr, 0, out);
+}
+kt_status kt_context_create_with_luts(const kt_config* cfg, int device, const float* bb_rgba,
+                                      const float* disk, uint32_t lut_n, kt_context** out) {
+    if (!bb_rgba || !disk) return fail(KT_ERR_INVALID_ARG, "LUT pointer is NULL");
+    return create_impl(cfg, device, bb_rgba, disk, lut_n, out);
+}
+void kt_context_destroy(kt_context* ctx) { destroy_ctx(ctx); }
+kt_status kt_context_params(const kt_context* ctx, kt_kerr_params* out) {
+    if (!ctx || !out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    *out = ctx->params;
+    return KT_OK;
+}
+
+kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
+                   float* hdr_out, uint32_t* err_word) {
+    if (!ctx || !cam || !hdr_out || !err_word) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (schedule != KT_SCHED_PLAIN && schedule != KT_SCHED_WAVEFRONT) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
+    DeviceGuard g(ctx->device);
+    const cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), schedule, reinterpret_cast<float4*>(hdr_out),
+                                            err_word, ctx->queue, nullptr, ctx->block_x, ctx->block_y,
+                                            (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "trace launch");
+    return KT_OK;
+}
+
+kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
+                           float* hdr_out, uint32_t* err_word, kt_trace_stats* stats) {
+    if (!ctx || !cam || !hdr_out || !err_word || !stats) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (schedule != KT_SCHED_PLAIN && schedule != KT_SCHED_WAVEFRONT) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    KT_CUDA(cudaMemsetAsync(ctx->counters, 0, 8 * sizeof(unsigned long long), st), "clear counters");
+    cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), schedule, reinterpret_cast<float4*>(hdr_out),
+                                      err_word, ctx->queue, ctx->counters, ctx->block_x, ctx->block_y, st);
+    if (e != cudaSuccess) return cuda_fail(e, "trace launch");
+    unsigned long long h[8];
+    KT_CUDA(cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, st), "read counters");
+    KT_CUDA(cudaStreamSynchronize(st), "synchronise");
+    stats->rays = h[0];
+    stats->steps = h[1];
+    stats->attempts = h[2];
+    stats->rhs_evals = h[3];
+    stats->frozen_rays = h[4];
+    stats->fp64_steps = h[5];
+    return KT_OK;
+}
+
+kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom) {
+    if (!ctx || !hdr || !bloom) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    DeviceGuard g(ctx->device);
+    const cudaError_t e = ktd::launch_bloom_horizontal(ctx->post, reinterpret_cast<const float4*>(hdr),
+                                                       reinterpret_cast<float4*>(bloom), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "bloom launch");
+    return KT_OK;
+}
+
+kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const float* bloom, uint32_t* image_out) {
+    if (!ctx || !hdr || !image_out || (ctx->post.active && !bloom)) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    DeviceGuard g(ctx->device);
+    const cudaError_t e = ktd::launch_post_process(ctx->post, reinterpret_cast<const float4*>(hdr),
+                                                   reinterpret_cast<const float4*>(bloom), image_out,
+                                                   (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "post launch");
+    return KT_OK;
+}
+
+kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_t* image_out) {
+    if (!ctx || !hdr || !image_out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    DeviceGuard g(ctx->device);
+    const cudaError_t e = ktd::launch_post_fused(ctx->post, reinterpret_cast<const float4*>(hdr), image_out,
+                                                 (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "fused post launch");
+    return KT_OK;
+}
+
+}  // extern "C"
+
+// =========================================================================================
+// CudaRenderer mirror (src/renderer/mod.rs)
+// =========================================================================================
+struct kt_frame {
+    float* hdr = nullptr;
+    float* bloom = nullptr;
+    uint32_t* image = nullptr;
+    uint32_t* host_image = nullptr;  // pinned
+    uint32_t* err = nullptr;
+    uint32_t* host_err = nullptr;    // pinned, 2 words
+    cudaEvent_t ready = nullptr;
+    bool has_event = false;
+};
+
+struct kt_renderer {
+    kt_context* ctx = nullptr;
+    cudaStream_t stream = nullptr;   // the legacy default stream, like cudarc's default_stream()
+    kt_frame frames[2];
+    std::deque<uint32_t> pending;
+    uint32_t next_frame = 0;
+    int schedule = KT_SCHED_WAVEFRONT;
+};
+
+namespace {
+void destroy_renderer(kt_renderer* r) {
+    if (!r) return;
+    if (r->ctx) {
+        DeviceGuard g(r->ctx->device);
+        cudaDeviceSynchronize();
+        for (auto& f : r->frames) {
+            cudaFree(f.hdr);
+            cudaFree(f.bloom);
+            cudaFree(f.image);
+            cudaFree(f.err);
+            cudaFreeHost(f.host_image);
+            cudaFreeHost(f.host_err);
+            if (f.ready) cudaEventDestroy(f.ready);
+        }
+        destroy_ctx(r->ctx);
+    }
+    delete r;
+}
+}  // namespace
+
+extern "C" {
+
+kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
+    if (!out) return fail(KT_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    kt_renderer* r = new (std::nothrow) kt_renderer();
+    if (!r) return fail(KT_ERR_INVALID_ARG, "out of host memory");
+    kt_status st = kt_context_create(cfg, device, &r->ctx);
+    if (st != KT_OK) {
+        delete r;
+        return st;
+    }
+    DeviceGuard g(device);
+    const size_t px = (size_t)cfg->width * cfg->height;
+    for (auto& f : r->frames) {
+        cudaError_t e;
+        if ((e = cudaMalloc(&f.hdr, px * 4 * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&f.bloom, px * 4 * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&f.image, px * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMalloc(&f.err, 2 * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMallocHost(&f.host_image, px * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMallocHost(&f.host_err, 2 * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&f.ready, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaMemset(f.hdr, 0, px * 4 * sizeof(float))) != cudaSuccess ||
+            (e = cudaMemset(f.bloom, 0, px * 4 * sizeof(float))) != cudaSuccess ||
+            (e = cudaMemset(f.image, 0, px * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMemset(f.err, 0, 2 * sizeof(uint32_t))) != cudaSuccess) {
+            st = cuda_fail(e, "allocate frame buffers");
+            destroy_renderer(r);
+            return st;
+        }
+        f.host_err[0] = f.host_err[1] = 0;
+    }
+    *out = r;
+    return KT_OK;
+}
+
+kt_status kt_renderer_set_schedule(kt_renderer* r, int32_t schedule) {
+    if (!r) return fail(KT_ERR_INVALID_ARG, "renderer is NULL");
+    if (schedule != KT_SCHED_PLAIN && schedule != KT_SCHED_WAVEFRONT) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
+    r->schedule = schedule;
+    return KT_OK;
+}
+
+kt_status kt_renderer_submit_render(kt_renderer* r, const float cam_pos[3], const float fwd[3],
+                                    const float rgt[3], const float up[3], float fov_scale,
+                                    int32_t* submitted) {
+    if (!r || !cam_pos || !fwd || !rgt || !up) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (submitted) *submitted = 0;
+    if (r->pending.size() == 2) return KT_OK;
+    uint32_t idx = 2;
+    for (uint32_t off = 0; off < 2; ++off) {
+        const uint32_t cand = (r->next_frame + off) % 2;
+        bool busy = false;
+        for (uint32_t p : r->pending) busy = busy || p == cand;
+        if (!busy) {
+            idx = cand;
+            break;
+        }
+    }
+    if (idx == 2) return fail(KT_ERR_INVALID_ARG, "no free frame buffer");
+    kt_frame& f = r->frames[idx];
+    kt_camera cam;
+    for (int i = 0; i < 3; ++i) {
+        cam.cam_pos[i] = cam_pos[i];
+        cam.fwd[i] = fwd[i];
+        cam.rgt[i] = rgt[i];
+        cam.up[i] = up[i];
+    }
+    cam.fov_scale = fov_scale;
+    DeviceGuard g(r->ctx->device);
+    const size_t px = (size_t)r->ctx->cfg.width * r->ctx->cfg.height;
+    KT_CUDA(cudaMemsetAsync(f.err, 0, 2 * sizeof(uint32_t), r->stream), "clear LUT error flag");
+    kt_status st = kt_trace(r->ctx, r->stream, &cam, r->schedule, f.hdr, f.err);
+    if (st != KT_OK) return st;
+    KT_CUDA(cudaMemcpyAsync(f.host_err, f.err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream), "read LUT error flag");
+    st = kt_post_fused(r->ctx, r->stream, f.hdr, f.image);
+    if (st != KT_OK) return st;
+    KT_CUDA(cudaMemcpyAsync(f.host_image, f.image, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream), "copy image back");
+    KT_CUDA(cudaEventRecord(f.ready, r->stream), "record frame event");
+    f.has_event = true;
+    r->pending.push_back(idx);
+    r->next_frame = (idx + 1) % 2;
+    if (submitted) *submitted = 1;
+    return KT_OK;
+}
+
+kt_status kt_renderer_ready_frame(kt_renderer* r, uint32_t* index, const uint32_t** data, float* overflow_temp) {
+    if (!r || !index || !data) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (r->pending.empty()) return KT_ERR_NOT_READY;
+    const uint32_t idx = r->pending.front();
+    kt_frame& f = r->frames[idx];
+    if (!f.has_event) return KT_ERR_NOT_READY;
+    const cudaError_t q = cudaEventQuery(f.ready);
+    if (q == cudaErrorNotReady) return KT_ERR_NOT_READY;
+    if (q != cudaSuccess) return cuda_fail(q, "query frame event");
+    if (f.host_err[0] != 0) {
+        float t;
+        std::memcpy(&t, &f.host_err[1], sizeof t);
+        if (overflow_temp) *overflow_temp = t;
+        return fail(KT_ERR_LUT_OVERFLOW, "colour temperature above lut_max_temp: %g > %g", t, r->ctx->cfg.lut_max_temp);
+    }
+    *index = idx;
+    *data = f.host_image;
+    return KT_OK;
+}
+
+kt_status kt_renderer_finish_frame(kt_renderer* r, uint32_t index) {
+    if (!r) return fail(KT_ERR_INVALID_ARG, "renderer is NULL");
+    if (r->pending.empty()) return fail(KT_ERR_QUEUE_ORDER, "frame queue is empty");
+    if (r->pending.front() != index)
+        return fail(KT_ERR_QUEUE_ORDER, "frame queue out of order: expect=%u got=%u", r->pending.front(), index);
+    r->pending.pop_front();
+    r->frames[index].has_event = false;
+    return KT_OK;
+}
+
+kt_status kt_renderer_wait(kt_renderer* r) {
+    if (!r) return fail(KT_ERR_INVALID_ARG, "renderer is NULL");
+    for (uint32_t idx : r->pending) {
+        if (r->frames[idx].has_event) KT_CUDA(cudaEventSynchronize(r->frames[idx].ready), "wait for frame");
+    }
+    return KT_OK;
+}
+
+kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev) {
+    if (!r || !hdr_dev || index > 1) return fail(KT_ERR_INVALID_ARG, "bad argument");
+    *hdr_dev = r->frames[index].hdr;
+    return KT_OK;
+}
+
+void kt_renderer_destroy(kt_renderer* r) { destroy_renderer(r); }
+
+}  // extern "C"

@@ -1,0 +1,39 @@
+// kt_internal.h — launchers shared by the C-ABI layer (kt_host.cpp) and the kernels
+// translation unit (kt_kernels.cu).  Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kt_types.h"
+
+namespace ktd {
+
+// Bloom / post-process constants of one context (src/renderer/init.rs:43-73, mod.rs:533-542).
+struct PostParams {
+    int width, height;
+    int radius;       // ceil(bloom.radius)
+    float sigma;      // bloom.radius / 3
+    float intensity;
+    int active;       // enabled && radius > 0 && intensity > 0
+    int mode;         // stated-physics luminance threshold when 1
+    float threshold;
+};
+
+// Trace launch: schedule 0 = plain 2D grid (block bx x by), 1 = persistent wavefront.
+// precision 0 = FP32, 1 = mixed, 2 = FP64.  queue: one zero-initialised device word per launch
+// (reset here on `stream`).  ctr: optional 6 x u64 device counters (counting kernels).
+cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
+                         uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx, int by,
+                         cudaStream_t stream);
+
+cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, float4* bloom,
+                                    cudaStream_t stream);
+cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const float4* bloom,
+                                uint32_t* image, cudaStream_t stream);
+cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image,
+                              cudaStream_t stream);
+
+// Resident blocks of the wavefront kernel for this scene's precision (occupancy query).
+int wavefront_grid(int precision, int device);
+
+}  // namespace ktd

@@ -1,0 +1,516 @@
+// kt_kernels.cu — trace and post-process kernels for sm_100a.
+//
+// Built with -use_fast_math, the flag set the reference compiles kernel.cu with
+// (config.yaml `cuda.use_fast_math: true`, src/renderer/init.rs:112-118), so that `/`, powf and
+// expf lower to the same instructions as in the reference.
+//
+// Trace kernels (replace trace_kernel, cuda/kernel.cu:88-142):
+//   trace_plain_kernel      one thread per pixel on a 2D grid of block_dim tiles; each thread
+//                           runs its spp rays to completion through the attempt state machine.
+//   trace_wavefront_kernel  persistent: one block per resident slot, each lane owns a pixel and
+//                           pulls a new one from a device work counter (warp-aggregated atomics)
+//                           as soon as its rays are done, so long rays never idle a whole warp.
+// Post kernels (replace bloom_horizontal / post_process, cuda/kernel.cu:144-251):
+//   bloom_h_kernel          horizontal normalised Gaussian from a shared-memory row segment
+//   post_v_kernel           vertical Gaussian from a shared-memory column tile + composite,
+//                           ACES, sRGB OETF, 0x00RRGGBB pack
+//   post_fused_kernel       both passes in one kernel, the horizontal result kept in shared
+//                           memory (no bloom buffer round trip through HBM)
+// All three post paths produce the reference's bits: same tap order, same weights, same
+// division and tone-map expressions.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kt_internal.h"
+#include "kt_ray.cuh"
+
+namespace ktd {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWavefrontBlock = 128;
+
+// ---- work counters (counting kernels only) -----------------------------------------------
+__device__ __forceinline__ void add_tally(unsigned long long* ctr, uint64_t rays, const Tally& t) {
+    atomicAdd(ctr + 0, (unsigned long long)rays);
+    atomicAdd(ctr + 1, (unsigned long long)t.steps);
+    atomicAdd(ctr + 2, (unsigned long long)t.attempts);
+    atomicAdd(ctr + 3, (unsigned long long)t.rhs);
+    atomicAdd(ctr + 4, (unsigned long long)t.frozen);
+    atomicAdd(ctr + 5, (unsigned long long)t.fp64);
+}
+__device__ __forceinline__ void tally_ray(Tally& acc, const Tally& ray) {
+    acc.steps += ray.steps;
+    acc.attempts += ray.attempts;
+    acc.rhs += ray.rhs;
+    acc.frozen += ray.frozen ? 1u : 0u;
+    acc.fp64 += ray.fp64;
+}
+
+// Runs one ray to completion (plain schedule).
+template <class R, bool COUNT>
+__device__ __forceinline__ void run_ray(int px, int py, int smp, const Scene& sc, const Camera& cam,
+                                        uint32_t* err, float acc[3], Tally& total) {
+    float dir[3];
+    pixel_ray(px, py, smp, sc, cam, dir);
+    RayRun<R> ry;
+    Tally tl;
+    tl.clear();
+    if (ray_start<R>(ry, cam, dir, sc)) {
+        while (!ray_advance<R, COUNT>(ry, sc, err, tl)) {
+        }
+    }
+    acc[0] += ry.col[0];
+    acc[1] += ry.col[1];
+    acc[2] += ry.col[2];
+    if (COUNT) tally_ray(total, tl);
+}
+
+template <class R, bool COUNT, int MAXT>
+__global__ void __launch_bounds__(MAXT) trace_plain_kernel(const Scene sc, const Camera cam,
+                                                           float4* __restrict__ hdr,
+                                                           uint32_t* __restrict__ err,
+                                                           unsigned long long* __restrict__ ctr) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= sc.width || py >= sc.height) return;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    Tally total;
+    total.clear();
+    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, COUNT>(px, py, smp, sc, cam, err, acc, total);
+    const float fs = sc.final_scale;
+    hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+    if (COUNT) add_tally(ctr, (uint64_t)sc.spp, total);
+}
+
+// Work unit -> pixel.  Units run over 16-row bands, 16-column tiles inside a band, row-major
+// inside a tile, so 32 consecutive units form a 16x2 patch (the footprint of one warp of the
+// reference's 16x16 blocks).  Exact bijection onto [0, W) x [0, H), partial tiles included.
+__device__ __forceinline__ void unit_to_pixel(unsigned u, int W, int H, int& px, int& py) {
+    const unsigned band_px = (unsigned)W * 16u;
+    const unsigned band = u / band_px;
+    const unsigned rem = u - band * band_px;
+    const int row0 = (int)band * 16;
+    const int hb = min(16, H - row0);
+    const unsigned tile_px = 16u * (unsigned)hb;
+    const unsigned tile = rem / tile_px;
+    const unsigned rem2 = rem - tile * tile_px;
+    const int col0 = (int)tile * 16;
+    const int wt = min(16, W - col0);
+    py = row0 + (int)(rem2 / (unsigned)wt);
+    px = col0 + (int)(rem2 % (unsigned)wt);
+}
+
+template <class R, bool COUNT, int MINB>
+__global__ void __launch_bounds__(kWavefrontBlock, MINB)
+    trace_wavefront_kernel(const Scene sc, const Camera cam, float4* __restrict__ hdr,
+                           uint32_t* __restrict__ err, unsigned* __restrict__ queue,
+                           unsigned long long* __restrict__ ctr) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lane_lt = (1u << lane) - 1u;
+    const unsigned n_units = (unsigned)sc.width * (unsigned)sc.height;
+    RayRun<R> ry;
+    int px = 0, py = 0, smp = 0;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    bool active = false;
+    bool open = true;
+    Tally tl, total;
+    tl.clear();
+    total.clear();
+    uint64_t rays = 0;
+
+    while (true) {
+        if (open) {
+            const unsigned need = __ballot_sync(kFull, !active);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                const unsigned cnt = (unsigned)__popc(need);
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(queue, cnt);
+                base = __shfl_sync(kFull, base, leader);
+                if (base + cnt >= n_units) open = false;
+                if (!active) {
+                    const unsigned u = base + (unsigned)__popc(need & lane_lt);
+                    if (u < n_units) {
+                        unit_to_pixel(u, sc.width, sc.height, px, py);
+                        acc[0] = acc[1] = acc[2] = 0.0f;
+                        // first sample with work; samples whose loop would not run add zero
+                        for (smp = 0; smp < sc.spp; ++smp) {
+                            float dir[3];
+                            pixel_ray(px, py, smp, sc, cam, dir);
+                            if (COUNT) tl.clear();
+                            if (ray_start<R>(ry, cam, dir, sc)) break;
+                        }
+                        if (smp < sc.spp) {
+                            active = true;
+                        } else {
+                            const float fs = sc.final_scale;
+                            hdr[py * sc.width + px] =
+                                make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+                            if (COUNT) rays += (uint64_t)sc.spp;
+                        }
+                    }
+                }
+            }
+        }
+        if (!__any_sync(kFull, active)) break;
+        if (active && ray_advance<R, COUNT>(ry, sc, err, tl)) {
+            acc[0] += ry.col[0];
+            acc[1] += ry.col[1];
+            acc[2] += ry.col[2];
+            if (COUNT) tally_ray(total, tl);
+            for (++smp; smp < sc.spp; ++smp) {
+                float dir[3];
+                pixel_ray(px, py, smp, sc, cam, dir);
+                if (COUNT) tl.clear();
+                if (ray_start<R>(ry, cam, dir, sc)) break;
+            }
+            if (smp >= sc.spp) {
+                const float fs = sc.final_scale;
+                hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+                if (COUNT) rays += (uint64_t)sc.spp;
+                active = false;
+            }
+        }
+    }
+    if (COUNT) add_tally(ctr, rays, total);
+}
+
+// ---- launch -------------------------------------------------------------------------------
+constexpr int kMinBlocksF32 = 4;   // 512 resident threads/SM -> <= 128 registers per thread
+constexpr int kMinBlocksF64 = 2;
+
+template <class R, bool COUNT>
+static cudaError_t launch_plain(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
+                                unsigned long long* ctr, int bx, int by, cudaStream_t st) {
+    const dim3 block(bx, by);
+    const dim3 grid((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
+    if (bx * by <= 256)
+        trace_plain_kernel<R, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
+    else
+        trace_plain_kernel<R, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
+    return cudaGetLastError();
+}
+
+template <class R, bool COUNT, int MINB>
+static cudaError_t launch_wave(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
+                               unsigned* queue, unsigned long long* ctr, cudaStream_t st) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, trace_wavefront_kernel<R, COUNT, MINB>, kWavefrontBlock, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    e = cudaMemsetAsync(queue, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    trace_wavefront_kernel<R, COUNT, MINB>
+        <<<sms * per_sm, kWavefrontBlock, 0, st>>>(sc, cam, hdr, err, queue, ctr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
+                         uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx, int by,
+                         cudaStream_t st) {
+    if (sc.width <= 0 || sc.height <= 0) return cudaSuccess;
+    const bool count = ctr != nullptr;
+    const bool f64 = sc.precision == 2;
+    if (schedule == 0) {
+        if (f64) return count ? launch_plain<double, true>(sc, cam, hdr, err, ctr, bx, by, st)
+                              : launch_plain<double, false>(sc, cam, hdr, err, ctr, bx, by, st);
+        return count ? launch_plain<float, true>(sc, cam, hdr, err, ctr, bx, by, st)
+                     : launch_plain<float, false>(sc, cam, hdr, err, ctr, bx, by, st);
+    }
+    if (f64) return count ? launch_wave<double, true, kMinBlocksF64>(sc, cam, hdr, err, queue, ctr, st)
+                          : launch_wave<double, false, kMinBlocksF64>(sc, cam, hdr, err, queue, ctr, st);
+    return count ? launch_wave<float, true, kMinBlocksF32>(sc, cam, hdr, err, queue, ctr, st)
+                 : launch_wave<float, false, kMinBlocksF32>(sc, cam, hdr, err, queue, ctr, st);
+}
+
+int wavefront_grid(int precision, int device) {
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    cudaError_t e = precision == 2
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_wavefront_kernel<double, false, kMinBlocksF64>, kWavefrontBlock, 0)
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_wavefront_kernel<float, false, kMinBlocksF32>, kWavefrontBlock, 0);
+    if (e != cudaSuccess) return 0;
+    return sms * per_sm;
+}
+
+// =========================================================================================
+// Post-processing
+// =========================================================================================
+
+// Gaussian tap weight (cuda/kernel.cu:48-53).
+__device__ __forceinline__ float tap_weight(int i, float sigma) {
+    const float t = (float)i;
+    const float den = 2.0f * sigma * sigma;
+    return __expf(-(t * t) / den);
+}
+
+// ACES filmic fit (cuda/kernel.cu:17-29) and sRGB OETF (cuda/kernel.cu:30-43).
+__device__ __forceinline__ float aces1(float x) {
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    return (x * (a * x + b)) / (x * (c * x + d) + e);
+}
+__device__ __forceinline__ float srgb1(float x) {
+    if (x <= 0.0031308f) return 12.92f * x;
+    return 1.055f * powf(x, 0.4166666666666667f) - 0.055f;
+}
+__device__ __forceinline__ uint32_t to_byte(float v) {
+    return (uint32_t)(unsigned char)__float2int_rn(__saturatef(v) * 255.0f);
+}
+__device__ __forceinline__ uint32_t tone_pack(float r, float g, float b) {
+    const float mr = srgb1(aces1(r)), mg = srgb1(aces1(g)), mb = srgb1(aces1(b));
+    return (to_byte(mr) << 16) | (to_byte(mg) << 8) | to_byte(mb);
+}
+
+// Bloom source (stated physics: only the part of the luminance above the threshold blooms).
+__device__ __forceinline__ float4 bloom_source(float4 c, const PostParams& pp) {
+    if (pp.mode != 1) return c;
+    const float L = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+    const float k = L > pp.threshold ? (L - pp.threshold) / L : 0.0f;
+    return make_float4(c.x * k, c.y * k, c.z * k, c.w);
+}
+
+constexpr int kRowSeg = 256;  // bloom_h: pixels per block
+
+// Horizontal pass: one block per 256-pixel row segment, the segment and its halo staged once.
+__global__ void __launch_bounds__(kRowSeg) bloom_h_kernel(const PostParams pp,
+                                                          const float4* __restrict__ hdr,
+                                                          float4* __restrict__ bloom) {
+    extern __shared__ float4 smem4[];
+    const int R = pp.radius;
+    float* w = reinterpret_cast<float*>(smem4 + kRowSeg + 2 * R);
+    const int y = blockIdx.y;
+    const int x0 = blockIdx.x * kRowSeg;
+    for (int i = threadIdx.x; i <= 2 * R; i += blockDim.x) w[i] = tap_weight(i - R, pp.sigma);
+    for (int j = threadIdx.x; j < kRowSeg + 2 * R; j += blockDim.x) {
+        const int gx = x0 - R + j;
+        smem4[j] = (gx >= 0 && gx < pp.width) ? bloom_source(__ldg(hdr + (size_t)y * pp.width + gx), pp)
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x;
+    if (x >= pp.width) return;
+    float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+    for (int i = -R; i <= R; ++i) {
+        const int sx = x + i;
+        if (sx < 0 || sx >= pp.width) continue;
+        const float wi = w[i + R];
+        const float4 c = smem4[threadIdx.x + R + i];
+        ax += c.x * wi;
+        ay += c.y * wi;
+        az += c.z * wi;
+        ws += wi;
+    }
+    if (ws > 0.0f) {
+        ax /= ws;
+        ay /= ws;
+        az /= ws;
+    }
+    bloom[(size_t)y * pp.width + x] = make_float4(ax, ay, az, 0.0f);
+}
+
+constexpr int kPostTX = 32, kPostTY = 8;
+
+// Vertical pass + composite + tone map: a 32-column strip of (8 + 2R) bloom rows in shared memory.
+__global__ void __launch_bounds__(kPostTX * kPostTY) post_v_kernel(const PostParams pp,
+                                                                    const float4* __restrict__ hdr,
+                                                                    const float4* __restrict__ bloom,
+                                                                    uint32_t* __restrict__ image) {
+    extern __shared__ float4 smem4[];
+    const int R = pp.active ? pp.radius : 0;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = blockIdx.x * kPostTX + tx;
+    const int y = blockIdx.y * kPostTY + ty;
+    float* w = reinterpret_cast<float*>(smem4 + (kPostTY + 2 * R) * kPostTX);
+    if (pp.active) {
+        const int tid = ty * kPostTX + tx;
+        for (int i = tid; i <= 2 * R; i += kPostTX * kPostTY) w[i] = tap_weight(i - R, pp.sigma);
+        for (int row = ty; row < kPostTY + 2 * R; row += kPostTY) {
+            const int gy = blockIdx.y * kPostTY + row - R;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (x < pp.width && gy >= 0 && gy < pp.height) v = __ldg(bloom + (size_t)gy * pp.width + x);
+            smem4[row * kPostTX + tx] = v;
+        }
+        __syncthreads();
+    }
+    if (x >= pp.width || y >= pp.height) return;
+    const size_t idx = (size_t)y * pp.width + x;
+    const float4 base = __ldg(hdr + idx);
+    float fr = base.x, fg = base.y, fb = base.z;
+    if (pp.active) {
+        float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+        for (int i = -R; i <= R; ++i) {
+            const int sy = y + i;
+            if (sy < 0 || sy >= pp.height) continue;
+            const float wi = w[i + R];
+            const float4 c = smem4[(ty + R + i) * kPostTX + tx];
+            ax += c.x * wi;
+            ay += c.y * wi;
+            az += c.z * wi;
+            ws += wi;
+        }
+        if (ws > 0.0f) {
+            ax /= ws;
+            ay /= ws;
+            az /= ws;
+        }
+        fr += ax * pp.intensity;
+        fg += ay * pp.intensity;
+        fb += az * pp.intensity;
+    }
+    image[idx] = tone_pack(fr, fg, fb);
+}
+
+// Fused post: tile of 64 x 32 output pixels.  Phase 1 computes the horizontal blur of the
+// (32 + 2R) source rows of the tile into shared memory, staging 8 HDR rows (with their
+// horizontal halo) at a time; phase 2 runs the vertical blur, composite and tone map.
+constexpr int kFuseTX = 64, kFuseTY = 32, kFuseChunk = 8, kFuseThreads = 256;
+
+__global__ void __launch_bounds__(kFuseThreads) post_fused_kernel(const PostParams pp,
+                                                                   const float4* __restrict__ hdr,
+                                                                   uint32_t* __restrict__ image) {
+    extern __shared__ float4 smem4[];
+    const int R = pp.radius;
+    const int segw = kFuseTX + 2 * R;
+    float4* stage = smem4;                                       // kFuseChunk x segw
+    float* hb = reinterpret_cast<float*>(stage + kFuseChunk * segw);  // (TY+2R) x TX x 3
+    float* w = hb + (kFuseTY + 2 * R) * kFuseTX * 3;             // 2R+1
+    const int x0 = blockIdx.x * kFuseTX, y0 = blockIdx.y * kFuseTY;
+    const int tid = threadIdx.x;
+    for (int i = tid; i <= 2 * R; i += kFuseThreads) w[i] = tap_weight(i - R, pp.sigma);
+    const int rows = kFuseTY + 2 * R;
+    for (int c0 = 0; c0 < rows; c0 += kFuseChunk) {
+        __syncthreads();
+        const int nrow = min(kFuseChunk, rows - c0);
+        for (int j = tid; j < nrow * segw; j += kFuseThreads) {
+            const int r = j / segw, cx = j - r * segw;
+            const int gy = y0 - R + c0 + r, gx = x0 - R + cx;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gy >= 0 && gy < pp.height && gx >= 0 && gx < pp.width)
+                v = bloom_source(__ldg(hdr + (size_t)gy * pp.width + gx), pp);
+            stage[j] = v;
+        }
+        __syncthreads();
+        for (int j = tid; j < nrow * kFuseTX; j += kFuseThreads) {
+            const int r = j / kFuseTX, cx = j - r * kFuseTX;
+            const int x = x0 + cx;
+            float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+            for (int i = -R; i <= R; ++i) {
+                const int sx = x + i;
+                if (sx < 0 || sx >= pp.width) continue;
+                const float wi = w[i + R];
+                const float4 c = stage[r * segw + cx + R + i];
+                ax += c.x * wi;
+                ay += c.y * wi;
+                az += c.z * wi;
+                ws += wi;
+            }
+            if (ws > 0.0f) {
+                ax /= ws;
+                ay /= ws;
+                az /= ws;
+            }
+            float* o = hb + ((c0 + r) * kFuseTX + cx) * 3;
+            o[0] = ax;
+            o[1] = ay;
+            o[2] = az;
+        }
+    }
+    __syncthreads();
+    for (int j = tid; j < kFuseTX * kFuseTY; j += kFuseThreads) {
+        const int ry = j / kFuseTX, cx = j - ry * kFuseTX;
+        const int x = x0 + cx, y = y0 + ry;
+        if (x >= pp.width || y >= pp.height) continue;
+        const size_t idx = (size_t)y * pp.width + x;
+        const float4 base = __ldg(hdr + idx);
+        float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+        for (int i = -R; i <= R; ++i) {
+            const int sy = y + i;
+            if (sy < 0 || sy >= pp.height) continue;
+            const float wi = w[i + R];
+            const float* c = hb + ((ry + R + i) * kFuseTX + cx) * 3;
+            ax += c[0] * wi;
+            ay += c[1] * wi;
+            az += c[2] * wi;
+            ws += wi;
+        }
+        if (ws > 0.0f) {
+            ax /= ws;
+            ay /= ws;
+            az /= ws;
+        }
+        image[idx] = tone_pack(base.x + ax * pp.intensity, base.y + ay * pp.intensity,
+                               base.z + az * pp.intensity);
+    }
+}
+
+// Tone map only (bloom inactive): one thread per pixel.
+__global__ void tonemap_kernel(const PostParams pp, const float4* __restrict__ hdr,
+                               uint32_t* __restrict__ image) {
+    const size_t n = (size_t)pp.width * pp.height;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float4 c = __ldg(hdr + i);
+        image[i] = tone_pack(c.x, c.y, c.z);
+    }
+}
+
+static size_t bloom_h_smem(int R) { return (size_t)(kRowSeg + 2 * R) * sizeof(float4) + (size_t)(2 * R + 1) * sizeof(float); }
+static size_t post_v_smem(int R) { return (size_t)(kPostTY + 2 * R) * kPostTX * sizeof(float4) + (size_t)(2 * R + 1) * sizeof(float); }
+static size_t post_fused_smem(int R) {
+    return (size_t)kFuseChunk * (kFuseTX + 2 * R) * sizeof(float4) +
+           (size_t)(kFuseTY + 2 * R) * kFuseTX * 3 * sizeof(float) + (size_t)(2 * R + 1) * sizeof(float);
+}
+constexpr size_t kSmemLimit = 200 * 1024;
+
+static cudaError_t set_smem(const void* fn, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, float4* bloom, cudaStream_t st) {
+    if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
+    const size_t sm = bloom_h_smem(pp.radius);
+    if (sm > kSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e = set_smem((const void*)bloom_h_kernel, sm);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((pp.width + kRowSeg - 1) / kRowSeg, pp.height);
+    bloom_h_kernel<<<grid, kRowSeg, sm, st>>>(pp, hdr, bloom);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const float4* bloom,
+                                uint32_t* image, cudaStream_t st) {
+    if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
+    const size_t sm = pp.active ? post_v_smem(pp.radius) : 0;
+    if (sm > kSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e = set_smem((const void*)post_v_kernel, sm);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((pp.width + kPostTX - 1) / kPostTX, (pp.height + kPostTY - 1) / kPostTY);
+    post_v_kernel<<<grid, dim3(kPostTX, kPostTY), sm, st>>>(pp, hdr, bloom, image);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image, cudaStream_t st) {
+    if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
+    if (!pp.active) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        tonemap_kernel<<<sms * 8, 256, 0, st>>>(pp, hdr, image);
+        return cudaGetLastError();
+    }
+    const size_t sm = post_fused_smem(pp.radius);
+    if (sm > kSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e = set_smem((const void*)post_fused_kernel, sm);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((pp.width + kFuseTX - 1) / kFuseTX, (pp.height + kFuseTY - 1) / kFuseTY);
+    post_fused_kernel<<<grid, kFuseThreads, sm, st>>>(pp, hdr, image);
+    return cudaGetLastError();
+}
+
+}  // namespace ktd

@@ -1,0 +1,368 @@
+// kt_ray.cuh — per-ray state machine of the geodesic tracer.
+//
+// The reference integrates one ray inside a single call (cuda/kerr_trace.cuh:4-240): an outer
+// loop over steps, an inner loop over DP5(4) attempts.  Here the same computation is cut at
+// attempt granularity: ray_advance() performs exactly one attempt and, when the attempt ends
+// the step (accepted, or max_attempts reached), commits it and runs the horizon / disk-plane /
+// escape tests.  A warp whose lanes hold rays at different attempt counts therefore keeps all
+// lanes busy on the expensive part (six RHS evaluations), and a lane whose ray has ended can be
+// refilled with a new ray without waiting for its neighbours.
+//
+// Arithmetic follows the reference expression by expression; the only behavioural addition is
+// retirement of rays whose state has become NaN (see ray_advance), which cannot change the
+// output: once y is NaN every later crossing / horizon / escape comparison is false and the
+// reference keeps iterating without touching the colour until max_steps.
+#pragma once
+#include "kt_device.cuh"
+
+namespace ktd {
+
+// scene constants in the integration type
+template <class R> __device__ __forceinline__ R sc_a(const Scene& s);
+template <class R> __device__ __forceinline__ R sc_aa(const Scene& s);
+template <class R> __device__ __forceinline__ R sc_M(const Scene& s);
+template <class R> __device__ __forceinline__ R sc_h0(const Scene& s);
+template <class R> __device__ __forceinline__ R sc_tol(const Scene& s);
+template <class R> __device__ __forceinline__ bool inside_horizon(R r, const Scene& s);
+template <class R> __device__ __forceinline__ bool beyond_escape(R r, const Scene& s);
+template <> __device__ __forceinline__ float sc_a<float>(const Scene& s) { return s.a; }
+template <> __device__ __forceinline__ float sc_aa<float>(const Scene& s) { return s.aa; }
+template <> __device__ __forceinline__ float sc_M<float>(const Scene& s) { return s.M; }
+template <> __device__ __forceinline__ float sc_h0<float>(const Scene& s) { return s.h0; }
+template <> __device__ __forceinline__ float sc_tol<float>(const Scene& s) { return s.base_tol; }
+template <> __device__ __forceinline__ bool inside_horizon<float>(float r, const Scene& s) { return r < s.horizon_lt; }
+template <> __device__ __forceinline__ bool beyond_escape<float>(float r, const Scene& s) { return r > s.escape_gt; }
+template <> __device__ __forceinline__ double sc_a<double>(const Scene& s) { return s.a_d; }
+template <> __device__ __forceinline__ double sc_aa<double>(const Scene& s) { return s.aa_d; }
+template <> __device__ __forceinline__ double sc_M<double>(const Scene& s) { return s.M_d; }
+template <> __device__ __forceinline__ double sc_h0<double>(const Scene& s) { return s.h0_d; }
+template <> __device__ __forceinline__ double sc_tol<double>(const Scene& s) { return s.base_tol_d; }
+template <> __device__ __forceinline__ bool inside_horizon<double>(double r, const Scene& s) { return r < s.horizon_d; }
+template <> __device__ __forceinline__ bool beyond_escape<double>(double r, const Scene& s) { return r > s.escape_d; }
+
+template <class R>
+struct RayRun {
+    R s[6];      // x, y, z, p_x, p_y, p_z
+    R k1[6];     // RHS at s (valid when have_k1)
+    R pt, kt, h, tol;
+    float col[3];
+    float tau;
+    int step;    // committed steps (the reference's loop index i)
+    int attempt; // attempts spent on the current step
+    bool have_k1;
+};
+
+// Work counters of one ray (only maintained by the counting kernels).
+struct Tally {
+    uint32_t steps, attempts, rhs, frozen, fp64;
+    __device__ __forceinline__ void clear() { steps = attempts = rhs = frozen = fp64 = 0; }
+};
+
+// Camera ray of sample `sample` of pixel (px, py) (cuda/kernel.cu:108-121): PCG jitter inside
+// the pixel, vertical field of view, aspect on u.  Stated-physics mode with one sample uses the
+// pixel centre.
+__device__ __forceinline__ void pixel_ray(int px, int py, int sample, const Scene& sc,
+                                          const Camera& cam, float dir[3]) {
+    float jx, jy;
+    if (sc.mode == 1 && sc.spp == 1) {
+        jx = 0.5f;
+        jy = 0.5f;
+    } else {
+        const uint32_t pidx = (uint32_t)(py * sc.width + px);
+        const uint64_t key = ((uint64_t)pidx << 32) | (uint64_t)(uint32_t)sample;
+        jx = unit_float(key);
+        jy = unit_float(key ^ 0xda3e39cb94b95bdbULL);
+    }
+    const float u = ((px + jx) * sc.inv_w_2 - 1.0f) * sc.aspect * cam.fov_scale;
+    const float v = (1.0f - (py + jy) * sc.inv_h_2) * cam.fov_scale;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dir[c] = u * cam.rgt[c] + v * cam.up[c] + cam.fwd[c];
+}
+
+// Null initialisation (cuda/kerr_trace.cuh:14-47): p_t from the null condition with the
+// "-sqrt" root, covariant spatial momentum p = n + 2 Hk l (k_t + l.n).  Returns false when
+// the step loop would not run at all.
+template <class R>
+__device__ __forceinline__ bool ray_start(RayRun<R>& ry, const Camera& cam, const float dir[3],
+                                          const Scene& sc) {
+    using O = Ops<R>;
+    const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
+    const R dx = (R)dir[0], dy = (R)dir[1], dz = (R)dir[2];
+    const R inv_n = O::rsq(dx * dx + dy * dy + dz * dz);
+    const R nx = dx * inv_n, ny = dy * inv_n, nz = dz * inv_n;
+    const R x = (R)cam.pos[0], y = (R)cam.pos[1], z = (R)cam.pos[2];
+    const R rho2 = O::fma(x, x, O::fma(y, y, z * z));
+    const R u = rho2 - aa;
+    const R s_term = O::sqrt_rn(O::fma(u, u, R(4) * aa * y * y));
+    const R r2 = R(0.5) * (u + s_term);
+    const R r = O::sqrt_rn(r2);
+    const R den = r2 + aa;
+    const R inv_den = O::fdiv(R(1), den);
+    const R lx = (r * x - a * z) * inv_den;
+    const R ly = O::fdiv(y, r);
+    const R lz = (r * z + a * x) * inv_den;
+    const R denH = O::fma(r2, r2, aa * y * y);
+    const R Hk = M * r2 * r * O::fdiv(R(1), denH);
+    const R ln = O::fma(lx, nx, O::fma(ly, ny, lz * nz));
+    const R g_tt = R(-1) + R(2) * Hk;
+    const R g_tn = R(2) * Hk * ln;
+    const R g_nn = R(1) + R(2) * Hk * ln * ln;
+    const R disc = g_tn * g_tn - g_tt * g_nn;
+    const R kt = (-g_tn - O::sqrt_rn(disc)) / g_tt;
+    const R pt = g_tt * kt + g_tn;
+    const R w = kt + ln;
+    ry.s[0] = x;
+    ry.s[1] = y;
+    ry.s[2] = z;
+    ry.s[3] = nx + R(2) * Hk * lx * w;
+    ry.s[4] = ny + R(2) * Hk * ly * w;
+    ry.s[5] = nz + R(2) * Hk * lz * w;
+    ry.pt = pt;
+    ry.kt = kt;
+    ry.h = sc_h0<R>(sc);
+    ry.tol = R(0);
+    ry.col[0] = ry.col[1] = ry.col[2] = 0.0f;
+    ry.tau = 1.0f;
+    ry.step = 0;
+    ry.attempt = 0;
+    ry.have_k1 = false;
+    return 0 < sc.max_steps && 1.0f > sc.cutoff_gt;
+}
+
+// Tolerance of the step starting at s (cuda/kerr_trace.cuh:67-73): scaled by the Kerr-Schild
+// potential from 5x far away down to 0 at Hk >= 0.3 (reference), or down to 1x (stated physics).
+template <class R>
+__device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
+    using O = Ops<R>;
+    const R aa = sc_aa<R>(sc), M = sc_M<R>(sc);
+    const R rc = ks_radius<R>(s[0], s[1], s[2], aa);
+    const R rc2 = rc * rc;
+    const R denH = O::fma(rc2, rc2, aa * s[1] * s[1]);
+    const R Hk = M * rc * rc2 * O::fdiv(R(1), denH);
+    R t = O::fdiv(Hk - lit<R>(0.05f, 0.05), lit<R>(0.3f, 0.3) - lit<R>(0.05f, 0.05));
+    t = O::minr(O::maxr(t, R(0)), R(1));
+    const R base = sc_tol<R>(sc);
+    if (sc.mode == 0) return base * (R(5) - R(5) * t);
+    return base * (R(5) - R(4) * t);
+}
+
+// Blackbody colour for the FP64 path (software interpolation, double coordinate).
+__device__ __forceinline__ float3 blackbody_rgb_d(double T, const Scene& sc, uint32_t* err) {
+    if (T > (double)sc.lut_max_temp) {
+        if (atomicCAS(err, 0u, 1u) == 0u) err[1] = __float_as_uint((float)T);
+        return make_float3(0.0f, 0.0f, 0.0f);
+    }
+    const double tn = T / (double)sc.lut_max_temp;
+    const double pos = tn * (double)(sc.lut_size - 1);
+    const double u = (pos + 0.5) / (double)sc.lut_size;
+    const float4 c = lut_lerp4<double>(sc.bb_lut, sc.lut_size, u);
+    return make_float3(c.x, c.y, c.z);
+}
+
+// Root of y(t) = 0 on the dense output (stated physics): safeguarded Newton with bisection
+// fallback, starting from the secant guess.  This is what cuda/kerr_trace.cuh:147-168 intends.
+template <class R>
+__device__ __forceinline__ R crossing_root(R y0, R y1, R k1, R k3, R k4, R k5, R k6, R k7, R h,
+                                           R t0) {
+    using O = Ops<R>;
+    R lo = R(0), hi = R(1), t = t0;
+    const bool neg0 = y0 < R(0);
+#pragma unroll 1
+    for (int it = 0; it < 12; ++it) {
+        const R yt = dense_eval<R>(y0, y1, k1, k3, k4, k5, k6, k7, h, t);
+        if (yt == R(0)) break;
+        if ((yt < R(0)) == neg0) lo = t; else hi = t;
+        const R dyt = dense_slope<R>(y0, y1, k1, k3, k4, k5, k6, k7, h, t);
+        R tn = dyt != R(0) ? t - yt / dyt : R(0.5) * (lo + hi);
+        if (!(tn > lo && tn < hi)) tn = R(0.5) * (lo + hi);
+        const R step = O::absr(tn - t);
+        t = tn;
+        if (step <= lit<R>(1e-7f, 1e-15)) break;
+    }
+    return t;
+}
+
+// Disk-plane crossing between prev and cur (cuda/kerr_trace.cuh:138-228): hit point on the
+// dense output, Novikov-Thorne disk test, redshift g, temperature from the disk LUT (with FBM
+// modulation), blackbody colour and alpha compositing.
+template <class R>
+__device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, const R* k1,
+                                               const R* k3, const R* k4, const R* k5,
+                                               const R* k6, const R* k7, R h, const Scene& sc,
+                                               uint32_t* err) {
+    using O = Ops<R>;
+    const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
+    const R y0 = prev[1], y1 = ry.s[1];
+    const R dy = y0 - y1;
+    R t = dy != R(0) ? O::fdiv(y0, dy) : R(0.5);
+    t = O::minr(O::maxr(t, R(0)), R(1));
+    if (sc.mode == 1) t = crossing_root<R>(y0, y1, k1[1], k3[1], k4[1], k5[1], k6[1], k7[1], h, t);
+    R hit[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        hit[c] = dense_eval<R>(prev[c], ry.s[c], k1[c], k3[c], k4[c], k5[c], k6[c], k7[c], h, t);
+    const R xh = hit[0], zh = hit[2], pxh = hit[3], pyh = hit[4], pzh = hit[5];
+    R rh = ks_radius<R>(xh, R(0), zh, aa);
+    const R r_in = (R)sc.disk_inner, r_out = (R)sc.disk_outer;
+    if (!(rh >= r_in && rh <= r_out)) return;
+    const R sqM = O::sqrt_rn(M), rs = O::sqrt_rn(rh);
+    const R disc = R(1) - R(3) * M / rh + R(2) * a * sqM / (rh * rs);
+    if (!(disc > R(0))) return;
+    const R omega = -sqM / (rh * rs + a * sqM);
+    const R r2h = rh * rh;
+    const R inv = O::fdiv(R(1), r2h + aa);
+    const R lx = (rh * xh - a * zh) * inv;
+    const R ly = R(0);
+    const R lz = (rh * zh + a * xh) * inv;
+    const R ldotp = O::fma(lx, pxh, O::fma(ly, pyh, lz * pzh));
+    const R ldotxi = lx * zh - lz * xh;
+    const R denH = r2h * r2h;
+    const R Hk = M * rh * r2h * O::fdiv(R(1), denH);
+    const R L = (zh * pxh - xh * pzh) + R(2) * Hk * ldotxi * (ldotp + ry.kt);
+    const R energy = -ry.pt;
+    const R l_over_e = O::fdiv(L, energy);
+    const R g = R(1) / (O::rsq(disc) * (R(1) - omega * l_over_e));
+    const R span = r_out - r_in;
+    const R u = span > R(0) ? (rh - r_in) / span : R(0);
+    R sampled;
+    if constexpr (sizeof(R) == 4) {
+        if (sc.mode == 0) sampled = tex1D<float>(sc.disk_tex, u);
+        else sampled = lut_lerp1<float>(sc.disk_lut, sc.lut_size, u);
+    } else {
+        sampled = lut_lerp1<double>(sc.disk_lut, sc.lut_size, u);
+    }
+    // CONFIG_DISK_TEMPERATURE_SCALE is a double literal in the reference: the product is double
+    double Td = sc.temp_scale * (double)sampled * (double)g;
+    R T = (R)Td;
+    if (sc.noise_enabled && sc.noise_detail > 0 && sc.noise_strength != 0.0f) {
+        R r_bl, sn_th, cs_th, phi;
+        const R inv_M = sizeof(R) == 4 ? (R)sc.inv_M : R(1) / M;
+        ks_to_bl<R>(xh, R(0), zh, a, aa, r_bl, sn_th, cs_th, phi);
+        rh = r_bl;  // the reference's ks_bl_from_xyz writes back into r_hit
+        const R r3 = rh * rh * rh;
+        const R om = R(1) / (a + O::sqrt_rn(r3 * inv_M));
+        R phase = phi + (R)sc.noise_winding * om;
+        if (sc.mode == 1) phase += (R)sc.noise_phase;
+        R sp, cp;
+        O::sincosr(phase, &sp, &cp);
+        const R nu = rh * cp * (R)sc.noise_scale;
+        const R nv = rh * sp * (R)sc.noise_scale;
+        const float nval = fbm2((float)nu, (float)nv, sc.noise_detail, sc.mode == 1 ? sc.noise_seed : 0u);
+        const float modulator = 1.0f + sc.noise_strength * (nval - 0.5f);
+        T *= (R)modulator;
+    }
+    if (O::isfiniter(T) && T > R(0)) {
+        float3 c;
+        if constexpr (sizeof(R) == 4) c = blackbody_rgb(T, sc, err);
+        else c = blackbody_rgb_d(T, sc, err);
+        const float luma = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+        const float luma_s = (float)((double)luma / sc.wl_step);
+        const float alpha = 1.0f - __expf(-luma_s * 0.5f);
+        ry.col[0] += c.x * alpha * ry.tau;
+        ry.col[1] += c.y * alpha * ry.tau;
+        ry.col[2] += c.z * alpha * ry.tau;
+        ry.tau *= (1.0f - alpha);
+    }
+}
+
+// One DP5(4) attempt; on the last attempt of a step, the commit and the per-step tests.
+// Returns true when the ray has finished (its colour is final).
+template <class R, bool COUNT>
+__device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint32_t* err,
+                                            Tally& tl) {
+    using O = Ops<R>;
+    using C = DP<R>;
+    const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
+    if (ry.attempt == 0) ry.tol = step_tolerance<R>(ry.s, sc);
+    if (!ry.have_k1) {
+        hamilton_rhs<R>(ry.s, ry.pt, a, aa, M, ry.k1);
+        ry.have_k1 = true;
+        if (COUNT) tl.rhs++;
+    }
+    const R h = ry.h;
+    const R* s = ry.s;
+    const R* k1 = ry.k1;
+    R y[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], nx[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * C::a21 * k1[c];
+    hamilton_rhs<R>(y, ry.pt, a, aa, M, k2);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a31 * k1[c] + C::a32 * k2[c]);
+    hamilton_rhs<R>(y, ry.pt, a, aa, M, k3);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a41 * k1[c] + C::a42 * k2[c] + C::a43 * k3[c]);
+    hamilton_rhs<R>(y, ry.pt, a, aa, M, k4);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        y[c] = s[c] + h * (C::a51 * k1[c] + C::a52 * k2[c] + C::a53 * k3[c] + C::a54 * k4[c]);
+    hamilton_rhs<R>(y, ry.pt, a, aa, M, k5);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        y[c] = s[c] + h * (C::a61 * k1[c] + C::a62 * k2[c] + C::a63 * k3[c] + C::a64 * k4[c] +
+                           C::a65 * k5[c]);
+    hamilton_rhs<R>(y, ry.pt, a, aa, M, k6);
+    // 5th-order solution; its stage-7 input is the same expression (a7j = b_j), so k7 is FSAL
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        nx[c] = s[c] + h * (C::b1 * k1[c] + C::b3 * k3[c] + C::b4 * k4[c] + C::b5 * k5[c] +
+                            C::b6 * k6[c]);
+    hamilton_rhs<R>(nx, ry.pt, a, aa, M, k7);
+    // max-norm of the embedded error, per-component scale tol * max(|y_i|, 1)
+    R e[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const R scale = ry.tol * O::maxr(O::absr(s[c]), R(1));
+        e[c] = O::absr(h * (C::e1 * k1[c] + C::e3 * k3[c] + C::e4 * k4[c] + C::e5 * k5[c] +
+                            C::e6 * k6[c] + C::e7 * k7[c])) / scale;
+    }
+    const R errv = O::maxr(O::maxr(O::maxr(e[0], e[1]), O::maxr(e[2], e[3])), O::maxr(e[4], e[5]));
+    const bool ok = errv <= R(1);
+    ry.h = h * lit<R>(0.9f, 0.9) * O::powr(errv, lit<R>(-0.2f, -0.2));
+    ry.attempt++;
+    if (COUNT) {
+        tl.attempts++;
+        tl.rhs += 6;
+    }
+    if (!ok && ry.attempt < sc.max_attempts) return false;  // retry; k1 stays valid at s
+
+    // commit (also when every attempt was rejected: cuda/kerr_trace.cuh:123-134)
+    R prev[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        prev[c] = ry.s[c];
+        ry.s[c] = nx[c];
+    }
+    ry.attempt = 0;
+    if (COUNT) tl.steps++;
+    if (O::isnanr(ry.s[1])) {  // frozen: no later comparison can succeed (see file comment)
+        if (COUNT) tl.frozen = 1;
+        return true;
+    }
+    const R r_now = ks_radius<R>(ry.s[0], ry.s[1], ry.s[2], aa);
+    if (inside_horizon<R>(r_now, sc)) return true;
+    if ((prev[1] < R(0) && ry.s[1] >= R(0)) || (prev[1] > R(0) && ry.s[1] <= R(0)))
+        shade_crossing<R>(ry, prev, ry.k1, k3, k4, k5, k6, k7, h, sc, err);
+    if (ok) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ry.k1[c] = k7[c];
+        ry.have_k1 = true;
+    } else {
+        ry.have_k1 = false;
+    }
+    if (beyond_escape<R>(r_now, sc)) {
+        R ke[6];
+        hamilton_rhs<R>(ry.s, ry.pt, a, aa, M, ke);
+        if (COUNT) tl.rhs++;
+        const R inv = O::rsq(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
+        const float sky = sky_value((float)(ke[0] * inv), (float)(ke[1] * inv), (float)(ke[2] * inv),
+                                    ry.tau, sc);
+        ry.col[0] += sky;
+        ry.col[1] += sky;
+        ry.col[2] += sky;
+        return true;
+    }
+    ry.step++;
+    return !(ry.step < sc.max_steps && ry.tau > sc.cutoff_gt);
+}
+
+}  // namespace ktd

@@ -1,0 +1,140 @@
+"""Named scenes: the benchmark configurations and the small parity scenes.
+
+Each function returns ``(KtConfig, KtCamera)``.  Values the benchmark description leaves open
+are fixed here and documented in DESIGN.md ("Workloads").
+
+  c1   256x256, FOV 30, r_obs 50, inclination 80, a = 0.9, tolerance 1e-8, h0 0.1,
+       20000 steps, horizon at 1.01 r_h, escape 1000, disk to 20 M, 256-entry LUTs over
+       380-780 nm in 5 nm steps, peak disk temperature 1e7 K, no noise, no bloom.
+  c2   1920x1080, FOV 25, r_obs 100, inclination 85, a = 0.998, tolerance 1e-6, 20000 steps,
+       disk to 30 M, FBM noise with 5 octaves, bloom radius 24 (sigma 8), ACES + sRGB.
+  t1   96x64 general parity scene (2 spp, noise, bloom radius 6) - seconds on the oracle.
+  t2   80x48 parity scene aimed at the sky grid and rejected steps (max_attempts 1).
+"""
+from __future__ import annotations
+
+from . import KtCamera, KtConfig, build_kerr_params, config_default, generate_disk_lut, orbit_camera
+
+
+def _peak_scale(cfg: KtConfig, peak_temp: float) -> float:
+    """disk_temperature_scale that puts the largest disk-LUT entry at `peak_temp` kelvin (the
+    reference scales an un-normalised f^(1/4), src/renderer/utils.rs:172-201)."""
+    lut = generate_disk_lut(build_kerr_params(cfg), cfg.disk_outer_radius, cfg.lut_size)
+    return float(peak_temp / float(lut.max()))
+
+
+def _horizon_eps(cfg: KtConfig, factor: float) -> float:
+    return float(build_kerr_params(cfg).rh * factor)
+
+
+def c1() -> tuple[KtConfig, KtCamera]:
+    c = config_default()
+    c.width, c.height = 256, 256
+    c.spp = 1
+    c.spin, c.mass = 0.9, 1.0
+    c.tolerance = 1e-8
+    c.initial_step = 0.1
+    c.max_steps = 20000
+    c.max_attempts = 3
+    c.escape_radius = 1000.0
+    c.horizon_epsilon = _horizon_eps(c, 0.01)
+    c.disk_outer_radius = 20.0
+    c.lut_size = 256
+    c.wavelength_start, c.wavelength_end, c.wavelength_step = 380.0, 780.0, 5.0
+    c.lut_max_temp = 4e7
+    c.disk_temperature_scale = _peak_scale(c, 1e7)
+    c.noise_enabled = 0
+    c.bloom_enabled = 0
+    c.exposure_scale = 1.0
+    return c, orbit_camera(50.0, 80.0, 30.0)
+
+
+def c2() -> tuple[KtConfig, KtCamera]:
+    c = config_default()
+    c.width, c.height = 1920, 1080
+    c.spp = 1
+    c.spin, c.mass = 0.998, 1.0
+    c.tolerance = 1e-6
+    c.initial_step = 0.1
+    c.max_steps = 20000
+    c.max_attempts = 3
+    c.escape_radius = 1000.0
+    c.horizon_epsilon = _horizon_eps(c, 0.01)
+    c.disk_outer_radius = 30.0
+    c.lut_size = 4096
+    c.wavelength_start, c.wavelength_end, c.wavelength_step = 380.0, 720.0, 10.0
+    c.lut_max_temp = 1e5
+    c.disk_temperature_scale = _peak_scale(c, 1e4)
+    c.exposure_scale = 3e-3
+    c.noise_enabled, c.noise_detail = 1, 5
+    c.noise_scale, c.noise_strength, c.noise_winding = 0.1, 0.6, 50.0
+    c.noise_seed, c.noise_phase = 42, 0.0
+    c.bloom_enabled, c.bloom_radius, c.bloom_intensity = 1, 24.0, 0.5
+    c.bloom_threshold = 1.0
+    return c, orbit_camera(100.0, 85.0, 25.0)
+
+
+def t1() -> tuple[KtConfig, KtCamera]:
+    c = config_default()
+    c.width, c.height = 96, 64
+    c.spp = 2
+    c.spin, c.mass = 0.9, 1.0
+    c.tolerance = 1e-5
+    c.initial_step = 0.5
+    c.max_steps = 3000
+    c.escape_radius = 200.0
+    c.horizon_epsilon = _horizon_eps(c, 0.01)
+    c.disk_outer_radius = 25.0
+    c.lut_size = 256
+    c.lut_max_temp = 1e5
+    c.disk_temperature_scale = _peak_scale(c, 1.2e4)
+    c.exposure_scale = 3e-3
+    c.noise_enabled, c.noise_detail = 1, 3
+    c.bloom_enabled, c.bloom_radius, c.bloom_intensity = 1, 6.0, 0.5
+    return c, orbit_camera(30.0, 75.0, 40.0)
+
+
+def t2() -> tuple[KtConfig, KtCamera]:
+    c = config_default()
+    c.width, c.height = 80, 48
+    c.spp = 1
+    c.spin, c.mass = -0.8, 1.0
+    c.tolerance = 2e-5
+    c.initial_step = 1.0
+    c.max_steps = 1500
+    c.max_attempts = 1
+    c.escape_radius = 120.0
+    c.horizon_epsilon = 5e-7
+    c.disk_outer_radius = 18.0
+    c.lut_size = 128
+    c.lut_max_temp = 1e5
+    c.disk_temperature_scale = _peak_scale(c, 9e3)
+    c.exposure_scale = 3e-3
+    c.sky_grid_divisions = 12
+    c.sky_line_thickness = 2e-2
+    c.noise_enabled = 0
+    c.bloom_enabled, c.bloom_radius, c.bloom_intensity = 1, 3.0, 0.8
+    return c, orbit_camera(40.0, 60.0, 70.0, azimuth_deg=30.0)
+
+
+SCENES = {"c1": c1, "c2": c2, "t1": t1, "t2": t2}
+
+
+def scene(name: str) -> tuple[KtConfig, KtCamera]:
+    return SCENES[name]()
+
+
+def scaled(cfg: KtConfig, width: int, height: int) -> KtConfig:
+    """Same scene at another resolution (everything else, including the defines, unchanged)."""
+    c = cfg.copy()
+    c.width, c.height = width, height
+    return c
+
+
+def rays(cfg: KtConfig) -> int:
+    return int(cfg.width) * int(cfg.height) * int(cfg.spp)
+
+
+def camera_list(cam: KtCamera) -> list[float]:
+    return [*cam.cam_pos, *cam.fwd, *cam.rgt, *cam.up]
+

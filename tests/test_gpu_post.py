@@ -1,0 +1,70 @@
+"""Post-processing on the GPU: the product's bloom / post / fused kernels against the reference's
+bloom_horizontal + post_process (oracle/_ref) on identical HDR input — bit-identical bloom
+buffers and 0x00RRGGBB images — and against the oracle's double-precision post (±1 per byte)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import kerrtrace_b200 as kt
+from kerrtrace_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _bloom_consts(cfg):
+    radius = int(np.ceil(np.float32(cfg.bloom_radius))) if cfg.bloom_radius > 0 else 0
+    sigma = float(np.float32(np.float32(cfg.bloom_radius) / np.float32(3.0)))
+    active = int(bool(cfg.bloom_enabled) and radius > 0 and cfg.bloom_intensity > 0)
+    return radius, sigma, active
+
+
+def _hdr_input(torch, cfg, seed):
+    """Synthetic HDR with a wide dynamic range, exact zeros, NaN-free."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    n = cfg.width * cfg.height
+    base = torch.rand((n, 4), generator=g) ** 6 * 20.0
+    base[torch.rand(n, generator=g) < 0.2] = 0.0
+    base[:, 3] = 1.0
+    return base.cuda()
+
+
+@pytest.mark.parametrize("name,size,radius", [("t1", None, None), ("t2", None, None), ("c2", (333, 190), None),
+                                              ("c2", (64, 40), 48.0), ("t1", (50, 70), 0.0)])
+def test_post_bit_identical_to_reference(cuda, orc, name, size, radius):
+    cfg, _ = workloads.scene(name)
+    if size:
+        cfg = workloads.scaled(cfg, *size)
+    if radius is not None:
+        cfg.bloom_radius = radius
+    R, sigma, active = _bloom_consts(cfg)
+    hdr = _hdr_input(cuda, cfg, 7)
+    n = cfg.width * cfg.height
+    ctx = kt.Context(cfg)
+    ref = orc.RefKernel(name)
+    bloom_o = cuda.zeros((n, 4), device="cuda")
+    bloom_r = cuda.zeros((n, 4), device="cuda")
+    img_o = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    img_f = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    img_r = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    if active:
+        ctx.bloom_horizontal(hdr.data_ptr(), bloom_o.data_ptr())
+        ref.bloom(hdr.data_ptr(), bloom_r.data_ptr(), cfg, R, sigma, active)
+    ctx.post_process(hdr.data_ptr(), bloom_o.data_ptr(), img_o.data_ptr())
+    ctx.post_fused(hdr.data_ptr(), img_f.data_ptr())
+    ref.post(hdr.data_ptr(), bloom_r.data_ptr(), img_r.data_ptr(), cfg, R, sigma, cfg.bloom_intensity, active)
+    cuda.cuda.synchronize()
+    bo, br = bloom_o.cpu().numpy(), bloom_r.cpu().numpy()
+    io, i_f, ir = (t.cpu().numpy().view(np.uint32) for t in (img_o, img_f, img_r))
+    if active:
+        assert np.array_equal(bo.view(np.uint32), br.view(np.uint32))
+    assert np.array_equal(io, ir)
+    assert np.array_equal(i_f, ir)
+    assert np.all(ir >> 24 == 0)
+    # oracle (double precision) agrees within one code value per channel
+    exp = orc.post(hdr.cpu().numpy(), cfg.width, cfg.height, R if active else 0, sigma, cfg.bloom_intensity)
+    d = np.max(np.abs(np.stack([(ir >> s) & 255 for s in (16, 8, 0)]).astype(int) -
+                      np.stack([(exp >> s) & 255 for s in (16, 8, 0)]).astype(int)), axis=0)
+    assert d.max() <= 1, np.bincount(d)
+    ctx.close()
+    ref.close()

@@ -1,0 +1,106 @@
+"""Trace kernels on the GPU: parity with the reference's own kernel.cu (compiled from source into
+oracle/_ref) and with the CPU oracle, schedule equivalence, counters and the LUT error word."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import kerrtrace_b200 as kt
+from kerrtrace_b200 import workloads
+from tests.helpers import compare_hdr, run_ours, run_ref
+
+pytestmark = pytest.mark.gpu
+
+# scene name -> resolution used in the test (defines identical to the full scene)
+CASES = {"t1": None, "t2": None, "c1": (128, 128), "c2": (320, 180)}
+
+
+def scene_at(name):
+    cfg, cam = workloads.scene(name)
+    if CASES[name]:
+        cfg = workloads.scaled(cfg, *CASES[name])
+    return cfg, cam
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_plain_and_wavefront_bit_identical(cuda, name):
+    cfg, cam = scene_at(name)
+    a, ea, _, ctx = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    b, eb, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_WAVEFRONT, ctx=ctx)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(ea, eb)
+    assert np.all(a[:, 3] == 1.0)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_matches_reference_kernel(cuda, name):
+    """Plain FP32 path vs the reference kernel: within 1e-3 relative on HDR RGB and identical
+    pixel classes away from silhouette pixels (the parity bar of the drop-in)."""
+    cfg, cam = scene_at(name)
+    ours, err_o, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_WAVEFRONT)
+    ref, err_r = run_ref(cuda, name, cfg, cam)
+    r = compare_hdr(ours, ref, cfg.width, cfg.height)
+    print(name, r)
+    assert r["class_mismatch_inner"] == 0, r
+    assert r["over_tol_inner"] == 0, r
+    assert r["over_tol_all"] <= max(2, 0.005 * r["n"]), r
+    assert np.array_equal(err_o, err_r)
+
+
+@pytest.mark.parametrize("name", ["t1", "c1"])
+def test_counters(cuda, name):
+    cfg, cam = scene_at(name)
+    _, _, st, ctx = run_ours(cuda, cfg, cam, kt.SCHED_WAVEFRONT, counted=True)
+    _, _, sp, _ = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN, counted=True, ctx=ctx)
+    assert st.rays == cfg.width * cfg.height * cfg.spp
+    for f in ("rays", "steps", "attempts", "rhs_evals", "frozen_rays"):
+        assert getattr(st, f) == getattr(sp, f), f
+    assert st.attempts >= st.steps > 0
+    assert 6 * st.attempts <= st.rhs_evals <= 7 * st.attempts + st.rays
+
+
+def test_matches_oracle_f32_and_f64(cuda, orc):
+    """GPU FP32 vs the CPU oracle (f32 emulation and f64) on the small scenes."""
+    for name in ("t1", "t2"):
+        cfg, cam = scene_at(name)
+        ours, _, _, _ = run_ours(cuda, cfg, cam)
+        for prec in (0, 2):
+            exp, _, _ = orc.Scene(cfg, cam, tex_mode=1).render(prec)
+            r = compare_hdr(ours, exp, cfg.width, cfg.height, rtol=1e-2)
+            print(name, prec, r)
+            assert r["class_mismatch_inner"] <= 0.002 * r["n"], r
+            assert r["over_tol_inner"] <= 0.01 * r["n"], r
+
+
+def test_lut_overflow_sets_error_word(cuda):
+    cfg, cam = scene_at("t1")
+    cfg.lut_max_temp = 2000.0  # far below the disk temperatures
+    ours, err, _, _ = run_ours(cuda, cfg, cam)
+    ref, err_r = run_ref(cuda, "t1", cfg, cam)
+    assert err[0] == 1 and err_r[0] == 1
+    t = err[1:2].view(np.float32)[0]
+    assert t > cfg.lut_max_temp
+    r = compare_hdr(ours, ref, cfg.width, cfg.height)
+    assert r["over_tol_inner"] == 0, r
+
+
+def test_fp64_spec_matches_f64_oracle(cuda, orc):
+    """Stated-physics FP64 GPU path vs the f64 oracle in the same mode."""
+    cfg, cam = scene_at("t1")
+    cfg.mode, cfg.precision = kt.MODE_SPEC, kt.PREC_FP64
+    ours, _, _, _ = run_ours(cuda, cfg, cam)
+    exp, _, _ = orc.Scene(cfg, cam, tex_mode=0).render(2)
+    r = compare_hdr(ours, exp, cfg.width, cfg.height, rtol=1e-4)
+    print(r)
+    assert r["class_mismatch_inner"] == 0, r
+    assert r["over_tol_inner"] <= 0.002 * r["n"], r
+
+
+def test_block_dims(cuda):
+    cfg, cam = scene_at("t2")
+    base, _, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    for bx, by in ((8, 8), (32, 8), (32, 32), (7, 5)):
+        c = cfg.copy()
+        c.block_dim[0], c.block_dim[1] = bx, by
+        out, _, _, _ = run_ours(cuda, c, cam, kt.SCHED_PLAIN)
+        assert np.array_equal(out.view(np.uint32), base.view(np.uint32)), (bx, by)
