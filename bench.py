@@ -48,55 +48,64 @@ def parse():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--size", default=None, help="WxH override of the scene resolution (same scene otherwise)")
     return ap.parse_args()
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """NVML sampling (every 5 ms, in a thread) of the SM clock and the clock-event reasons
+    during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_s: float = 0.005):
         self.dev = device_index
-        self.proc = None
-        self.path = Path(f"/tmp/kt_clocks_{os.getpid()}.csv")
+        self.period = period_s
+        self.samples = []
+        self._stop = None
+        self._thread = None
+        self.max_mhz = None
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        except Exception:  # no NVML: the summary says so
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    why = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    pw = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    self.samples.append((float(mhz), int(why), pw))
+                except Exception:
+                    pass
+                self._stop.wait(self.period)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self) -> dict:
-        rows = []
-        if self.path.exists():
-            for line in self.path.read_text().splitlines():
-                f = [x.strip() for x in line.split(",")]
-                if len(f) >= 9 and f[1].replace(".", "").isdigit():
-                    rows.append(f)
-            self.path.unlink(missing_ok=True)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(r[1]) for r in rows)
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
-                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()),
-                "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        sm = sorted(x[0] for x in self.samples)
+        reasons = sorted({name for _, why, _ in self.samples for bit, name in self.REASONS.items() if why & bit})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "power_w_max": round(max(x[2] for x in self.samples), 1), "samples": len(self.samples)}
 
 
 def dist_setup():
@@ -129,8 +138,11 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def rank_camera(kt, workloads, name, rank, world):
+def rank_camera(kt, workloads, name, rank, world, size=None):
     cfg, cam = workloads.scene(name)
+    if size:
+        w, h = (int(v) for v in size.lower().split("x"))
+        cfg = workloads.scaled(cfg, w, h)
     if world > 1 and rank > 0:
         r = math.sqrt(sum(c * c for c in cam.cam_pos))
         incl = math.degrees(math.acos(cam.cam_pos[1] / r))
@@ -140,27 +152,36 @@ def rank_camera(kt, workloads, name, rank, world):
 
 
 def cpu_baseline(cfg, cam, budget_s: float) -> dict:
-    """The CPU oracle (f64, reference semantics, all host cores) on a strided pixel sample."""
+    """The CPU oracle (f64, reference semantics, all host cores): whole frames of the same scene
+    until `budget_s` has elapsed, or a strided pixel sample when one frame would exceed it."""
     import numpy as np
 
     import oracle
     threads = os.cpu_count() or 1
     sc = oracle.Scene(cfg, cam, tex_mode=1)
     n = cfg.width * cfg.height
-    stride = 4096
-    t = 0.0
-    while True:
+    probe = np.arange(0, n, 64, dtype=np.int64)
+    t0 = time.perf_counter()
+    sc.render(2, pixels=probe, threads=threads)
+    est_frame = (time.perf_counter() - t0) * 64
+    if est_frame <= budget_s:
+        frames, t = 0, 0.0
+        while t < budget_s and frames < 20:
+            t0 = time.perf_counter()
+            sc.render(2, threads=threads)
+            t += time.perf_counter() - t0
+            frames += 1
+        rays = frames * n * cfg.spp
+        sample = f"f64 oracle, {frames} whole {cfg.width}x{cfg.height} frame(s) in {t:.2f} s"
+    else:
+        stride = max(1, int(math.ceil(est_frame / budget_s)))
         pix = np.arange(0, n, stride, dtype=np.int64)
         t0 = time.perf_counter()
         sc.render(2, pixels=pix, threads=threads)
         t = time.perf_counter() - t0
-        if t > budget_s / 4 or stride <= 16:
-            break
-        stride = max(16, int(stride * max(0.1, t / (budget_s / 2))) if t > 0 else stride // 8)
-    rays = len(pix) * cfg.spp
-    return {"value": rays / t / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
-            "sample": f"f64 oracle, every {stride}th pixel of the {cfg.width}x{cfg.height} frame "
-                      f"({len(pix)} pixels x {cfg.spp} spp) in {t:.2f} s"}
+        rays = len(pix) * cfg.spp
+        sample = f"f64 oracle, every {stride}th pixel of the {cfg.width}x{cfg.height} frame ({len(pix)} pixels) in {t:.2f} s"
+    return {"value": round(rays / t / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample}
 
 
 def run_ours(args, rank, world, local):
@@ -169,7 +190,7 @@ def run_ours(args, rank, world, local):
     import kerrtrace_b200 as kt
     from kerrtrace_b200 import flops, workloads
 
-    cfg, cam = rank_camera(kt, workloads, args.workload, rank, world)
+    cfg, cam = rank_camera(kt, workloads, args.workload, rank, world, args.size)
     sched = kt.SCHED_WAVEFRONT if args.schedule == "wavefront" else kt.SCHED_PLAIN
     ctx = kt.Context(cfg, local)
     n = cfg.width * cfg.height
@@ -281,7 +302,7 @@ def run_reference(args, rank, world, local):
 
     if rank != 0:
         return
-    cfg, cam = workloads.scene(args.workload)
+    cfg, cam = rank_camera(kt, workloads, args.workload, 0, 1, args.size)
     if not oracle.ref_lib_path(args.workload).exists():
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/libktref_{args.workload}.so not built"}))
         return

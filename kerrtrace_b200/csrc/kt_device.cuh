@@ -120,7 +120,12 @@ __device__ __forceinline__ R ks_radius(R x, R y, R z, R aa) {
 // y = (x, y, z, p_x, p_y, p_z); p_t = pt is conserved.  With the Kerr-Schild potential
 // Hk = M r^3 / (r^4 + a^2 y^2) and null vector l, the RHS is
 //   dx/dl = p - 2 Hk (l.p - pt) l,   dp/dl = dHk/dx (l.p - pt)^2 + 2 Hk (l.p - pt) d(l.p)/dx.
-template <class R>
+//
+// EXACT selects the y-derivative of r^2.  The reference writes d(r^2)/dy = y (1 + (u + 4a^2)/(2s))
+// (cuda/kerr_math.cuh:97); differentiating r^2 = (u + s)/2 with u = rho^2 - a^2 and
+// s^2 = u^2 + 4 a^2 y^2 gives y (1 + (u + 2a^2)/s).  Reference mode keeps the reference's
+// expression (the drop-in reproduces its images); stated-physics mode uses the exact one.
+template <class R, bool EXACT>
 __device__ __forceinline__ void hamilton_rhs(const R* __restrict__ st, R pt, R a, R aa, R M,
                                              R* __restrict__ d) {
     using O = Ops<R>;
@@ -135,7 +140,8 @@ __device__ __forceinline__ void hamilton_rhs(const R* __restrict__ st, R pt, R a
     const R r = r2 * inv_r;
     // gradient of r via r^2
     const R g2x = x * (R(1) + u * inv_s);
-    const R g2y = y * (R(1) + (u + R(4) * aa) * (R(0.5) * inv_s));
+    const R g2y = EXACT ? y * (R(1) + (u + R(2) * aa) * inv_s)
+                        : y * (R(1) + (u + R(4) * aa) * (R(0.5) * inv_s));
     const R g2z = z * (R(1) + u * inv_s);
     const R half_inv_r = R(0.5) * inv_r;
     const R rx = g2x * half_inv_r;
@@ -226,61 +232,73 @@ __device__ __forceinline__ R dense_slope(R y0, R y1, R k1, R k3, R k4, R k5, R k
 }
 
 // ---- gradient noise / FBM (cuda/kerr_math.cuh:172-179, 220-281) ----------------------------
-__device__ __forceinline__ float smooth5(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
-__device__ __forceinline__ float mixf(float a, float b, float t) { return fmaf(t, b - a, a); }
-__device__ __forceinline__ float2 lattice_gradient(int ix, int iy, unsigned seed) {
+// Float instantiation = the reference's arithmetic; double instantiation = the same lattice
+// (same PCG hash, same float-rounded gradient angle) evaluated in double.
+template <class R> __device__ __forceinline__ R smooth5(R t) { return t * t * t * (t * (t * R(6) - R(15)) + R(10)); }
+template <class R> __device__ __forceinline__ R mixr(R a, R b, R t) { return Ops<R>::fma(t, b - a, a); }
+template <class R>
+__device__ __forceinline__ void lattice_gradient(int ix, int iy, unsigned seed, R& gx, R& gy) {
     const uint64_t key = (((uint64_t)(uint32_t)ix) << 32) | (uint64_t)(uint32_t)iy;
     const uint32_t hsh = pcg_hash(key ^ (uint64_t)seed);
     constexpr float kAngle = 6.283185307f * 2.3283064365386963e-10f;
-    const float ang = (float)hsh * kAngle;
-    float sn, cs;
-    __sincosf(ang, &sn, &cs);
-    return make_float2(cs, sn);
+    const R ang = (R)((float)hsh) * (R)kAngle;
+    Ops<R>::sincosr(ang, &gy, &gx);
 }
-__device__ __forceinline__ float gradient_noise2(float u, float v, unsigned seed) {
-    const int ix0 = __float2int_rd(u);
-    const int iy0 = __float2int_rd(v);
+template <class R> __device__ __forceinline__ int floor_int(R v);
+template <> __device__ __forceinline__ int floor_int<float>(float v) { return __float2int_rd(v); }
+template <> __device__ __forceinline__ int floor_int<double>(double v) { return __double2int_rd(v); }
+template <class R>
+__device__ __forceinline__ R gradient_noise2(R u, R v, unsigned seed) {
+    const int ix0 = floor_int<R>(u);
+    const int iy0 = floor_int<R>(v);
     const int ix1 = ix0 + 1, iy1 = iy0 + 1;
-    const float fx = u - (float)ix0;
-    const float fy = v - (float)iy0;
-    const float2 g00 = lattice_gradient(ix0, iy0, seed);
-    const float2 g10 = lattice_gradient(ix1, iy0, seed);
-    const float2 g01 = lattice_gradient(ix0, iy1, seed);
-    const float2 g11 = lattice_gradient(ix1, iy1, seed);
-    const float n00 = g00.x * fx + g00.y * fy;
-    const float n10 = g10.x * (fx - 1.0f) + g10.y * fy;
-    const float n01 = g01.x * fx + g01.y * (fy - 1.0f);
-    const float n11 = g11.x * (fx - 1.0f) + g11.y * (fy - 1.0f);
-    const float uf = smooth5(fx);
-    const float vf = smooth5(fy);
-    const float m0 = mixf(n00, n10, uf);
-    const float m1 = mixf(n01, n11, uf);
-    return mixf(m0, m1, vf);
+    const R fx = u - (R)ix0;
+    const R fy = v - (R)iy0;
+    R g00x, g00y, g10x, g10y, g01x, g01y, g11x, g11y;
+    lattice_gradient<R>(ix0, iy0, seed, g00x, g00y);
+    lattice_gradient<R>(ix1, iy0, seed, g10x, g10y);
+    lattice_gradient<R>(ix0, iy1, seed, g01x, g01y);
+    lattice_gradient<R>(ix1, iy1, seed, g11x, g11y);
+    const R n00 = g00x * fx + g00y * fy;
+    const R n10 = g10x * (fx - R(1)) + g10y * fy;
+    const R n01 = g01x * fx + g01y * (fy - R(1));
+    const R n11 = g11x * (fx - R(1)) + g11y * (fy - R(1));
+    const R uf = smooth5<R>(fx);
+    const R vf = smooth5<R>(fy);
+    const R m0 = mixr<R>(n00, n10, uf);
+    const R m1 = mixr<R>(n01, n11, uf);
+    return mixr<R>(m0, m1, vf);
 }
-__device__ __forceinline__ float fbm2(float u, float v, int octaves, unsigned seed) {
-    if (octaves <= 0) return 0.5f;
-    float sum = 0.0f, amp = 1.0f, freq = 1.0f, amp_sum = 0.0f;
+template <class R>
+__device__ __forceinline__ R fbm2(R u, R v, int octaves, unsigned seed) {
+    if (octaves <= 0) return R(0.5);
+    R sum = R(0), amp = R(1), freq = R(1), amp_sum = R(0);
     for (int o = 0; o < octaves; ++o) {
-        sum += gradient_noise2(u * freq, v * freq, seed) * amp;
+        sum += gradient_noise2<R>(u * freq, v * freq, seed) * amp;
         amp_sum += amp;
-        amp *= 0.5f;
-        freq *= 2.0f;
+        amp *= R(0.5);
+        freq *= R(2);
     }
-    float val = amp_sum > 0.0f ? (sum / amp_sum) : 0.0f;
-    return val * 0.5f + 0.5f;
+    R val = amp_sum > R(0) ? (sum / amp_sum) : R(0);
+    return val * R(0.5) + R(0.5);
 }
 
 // ---- procedural sky grid (cuda/kerr_math.cuh:157-171) -----------------------------------
-__device__ __forceinline__ float sky_value(float dx, float dy, float dz, float tau, const Scene& sc) {
-    const float lon = atan2f(dz, dx);
-    const float lat = asinf(dy);
-    const float spacing = sc.sky_spacing;
-    const float thick = sc.sky_thickness;
-    const float dlon = fmodf(fabsf(lon), spacing);
-    const float dlat = fmodf(fabsf(lat), spacing);
+__device__ __forceinline__ float asin_r(float x) { return asinf(x); }
+__device__ __forceinline__ double asin_r(double x) { return asin(x); }
+__device__ __forceinline__ float fmod_r(float a, float b) { return fmodf(a, b); }
+__device__ __forceinline__ double fmod_r(double a, double b) { return fmod(a, b); }
+template <class R>
+__device__ __forceinline__ float sky_value(R dx, R dy, R dz, float tau, const Scene& sc) {
+    const R lon = Ops<R>::atan2r(dz, dx);
+    const R lat = asin_r(dy);
+    const R spacing = (R)sc.sky_spacing;
+    const R thick = (R)sc.sky_thickness;
+    const R dlon = fmod_r(Ops<R>::absr(lon), spacing);
+    const R dlat = fmod_r(Ops<R>::absr(lat), spacing);
     const bool on_line = (dlon < thick || dlon > (spacing - thick)) ||
                          (dlat < thick || dlat > (spacing - thick)) ||
-                         (fabsf(lat) < thick * 3.0f);
+                         (Ops<R>::absr(lat) < thick * R(3));
     return on_line ? (float)(sc.sky_intensity * (double)tau) : 0.0f;
 }
 
@@ -318,6 +336,7 @@ __device__ __forceinline__ float4 lut_lerp4(const float4* __restrict__ lut, int 
 
 // Blackbody colour of temperature T with the reference's overflow report
 // (cuda/kernel.cu:1-16): above lut_max_temp the first thread to notice records T.
+template <int MODE>
 __device__ __forceinline__ float3 blackbody_rgb(float T, const Scene& sc, uint32_t* err) {
     if (T > sc.lut_max_temp) {
         if (atomicCAS(err, 0u, 1u) == 0u) err[1] = __float_as_uint(T);
@@ -327,7 +346,7 @@ __device__ __forceinline__ float3 blackbody_rgb(float T, const Scene& sc, uint32
     const float pos = tn * (float)(sc.lut_size - 1);
     const float u = (pos + 0.5f) / (float)sc.lut_size;
     float4 c;
-    if (sc.mode == 0) c = tex1D<float4>(sc.bb_tex, u);
+    if (MODE == 0) c = tex1D<float4>(sc.bb_tex, u);
     else c = lut_lerp4<float>(sc.bb_lut, sc.lut_size, u);
     return make_float3(c.x, c.y, c.z);
 }

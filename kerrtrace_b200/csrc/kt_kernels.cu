@@ -47,16 +47,16 @@ __device__ __forceinline__ void tally_ray(Tally& acc, const Tally& ray) {
 }
 
 // Runs one ray to completion (plain schedule).
-template <class R, bool COUNT>
+template <class R, int MODE, bool COUNT>
 __device__ __forceinline__ void run_ray(int px, int py, int smp, const Scene& sc, const Camera& cam,
                                         uint32_t* err, float acc[3], Tally& total) {
     float dir[3];
-    pixel_ray(px, py, smp, sc, cam, dir);
+    pixel_ray<MODE>(px, py, smp, sc, cam, dir);
     RayRun<R> ry;
     Tally tl;
     tl.clear();
     if (ray_start<R>(ry, cam, dir, sc)) {
-        while (!ray_advance<R, COUNT>(ry, sc, err, tl)) {
+        while (!ray_advance<R, MODE, COUNT>(ry, sc, err, tl)) {
         }
     }
     acc[0] += ry.col[0];
@@ -65,7 +65,7 @@ __device__ __forceinline__ void run_ray(int px, int py, int smp, const Scene& sc
     if (COUNT) tally_ray(total, tl);
 }
 
-template <class R, bool COUNT, int MAXT>
+template <class R, int MODE, bool COUNT, int MAXT>
 __global__ void __launch_bounds__(MAXT) trace_plain_kernel(const Scene sc, const Camera cam,
                                                            float4* __restrict__ hdr,
                                                            uint32_t* __restrict__ err,
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(MAXT) trace_plain_kernel(const Scene sc, const
     float acc[3] = {0.0f, 0.0f, 0.0f};
     Tally total;
     total.clear();
-    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, COUNT>(px, py, smp, sc, cam, err, acc, total);
+    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total);
     const float fs = sc.final_scale;
     hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
     if (COUNT) add_tally(ctr, (uint64_t)sc.spp, total);
@@ -100,7 +100,7 @@ __device__ __forceinline__ void unit_to_pixel(unsigned u, int W, int H, int& px,
     px = col0 + (int)(rem2 % (unsigned)wt);
 }
 
-template <class R, bool COUNT, int MINB>
+template <class R, int MODE, bool COUNT, int MINB>
 __global__ void __launch_bounds__(kWavefrontBlock, MINB)
     trace_wavefront_kernel(const Scene sc, const Camera cam, float4* __restrict__ hdr,
                            uint32_t* __restrict__ err, unsigned* __restrict__ queue,
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
                         // first sample with work; samples whose loop would not run add zero
                         for (smp = 0; smp < sc.spp; ++smp) {
                             float dir[3];
-                            pixel_ray(px, py, smp, sc, cam, dir);
+                            pixel_ray<MODE>(px, py, smp, sc, cam, dir);
                             if (COUNT) tl.clear();
                             if (ray_start<R>(ry, cam, dir, sc)) break;
                         }
@@ -153,14 +153,14 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
             }
         }
         if (!__any_sync(kFull, active)) break;
-        if (active && ray_advance<R, COUNT>(ry, sc, err, tl)) {
+        if (active && ray_advance<R, MODE, COUNT>(ry, sc, err, tl)) {
             acc[0] += ry.col[0];
             acc[1] += ry.col[1];
             acc[2] += ry.col[2];
             if (COUNT) tally_ray(total, tl);
             for (++smp; smp < sc.spp; ++smp) {
                 float dir[3];
-                pixel_ray(px, py, smp, sc, cam, dir);
+                pixel_ray<MODE>(px, py, smp, sc, cam, dir);
                 if (COUNT) tl.clear();
                 if (ray_start<R>(ry, cam, dir, sc)) break;
             }
@@ -179,62 +179,68 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
 constexpr int kMinBlocksF32 = 4;   // 512 resident threads/SM -> <= 128 registers per thread
 constexpr int kMinBlocksF64 = 2;
 
-template <class R, bool COUNT>
+template <class R, int MODE, bool COUNT>
 static cudaError_t launch_plain(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
                                 unsigned long long* ctr, int bx, int by, cudaStream_t st) {
     const dim3 block(bx, by);
     const dim3 grid((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
     if (bx * by <= 256)
-        trace_plain_kernel<R, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
+        trace_plain_kernel<R, MODE, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
     else
-        trace_plain_kernel<R, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
+        trace_plain_kernel<R, MODE, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
     return cudaGetLastError();
 }
 
-template <class R, bool COUNT, int MINB>
+template <class R, int MODE, bool COUNT>
+static const void* wave_fn() {
+    return (const void*)trace_wavefront_kernel<R, MODE, COUNT, sizeof(R) == 4 ? kMinBlocksF32 : kMinBlocksF64>;
+}
+
+template <class R, int MODE, bool COUNT>
 static cudaError_t launch_wave(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
                                unsigned* queue, unsigned long long* ctr, cudaStream_t st) {
+    constexpr int MINB = sizeof(R) == 4 ? kMinBlocksF32 : kMinBlocksF64;
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, trace_wavefront_kernel<R, COUNT, MINB>, kWavefrontBlock, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_wavefront_kernel<R, MODE, COUNT, MINB>,
+                                                      kWavefrontBlock, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     e = cudaMemsetAsync(queue, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
-    trace_wavefront_kernel<R, COUNT, MINB>
+    trace_wavefront_kernel<R, MODE, COUNT, MINB>
         <<<sms * per_sm, kWavefrontBlock, 0, st>>>(sc, cam, hdr, err, queue, ctr);
     return cudaGetLastError();
+}
+
+template <class R, int MODE>
+static cudaError_t launch_typed(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
+                                uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx,
+                                int by, cudaStream_t st) {
+    if (schedule == 0)
+        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, bx, by, st)
+                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, bx, by, st);
+    return ctr ? launch_wave<R, MODE, true>(sc, cam, hdr, err, queue, ctr, st)
+               : launch_wave<R, MODE, false>(sc, cam, hdr, err, queue, ctr, st);
 }
 
 cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
                          uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx, int by,
                          cudaStream_t st) {
     if (sc.width <= 0 || sc.height <= 0) return cudaSuccess;
-    const bool count = ctr != nullptr;
-    const bool f64 = sc.precision == 2;
-    if (schedule == 0) {
-        if (f64) return count ? launch_plain<double, true>(sc, cam, hdr, err, ctr, bx, by, st)
-                              : launch_plain<double, false>(sc, cam, hdr, err, ctr, bx, by, st);
-        return count ? launch_plain<float, true>(sc, cam, hdr, err, ctr, bx, by, st)
-                     : launch_plain<float, false>(sc, cam, hdr, err, ctr, bx, by, st);
-    }
-    if (f64) return count ? launch_wave<double, true, kMinBlocksF64>(sc, cam, hdr, err, queue, ctr, st)
-                          : launch_wave<double, false, kMinBlocksF64>(sc, cam, hdr, err, queue, ctr, st);
-    return count ? launch_wave<float, true, kMinBlocksF32>(sc, cam, hdr, err, queue, ctr, st)
-                 : launch_wave<float, false, kMinBlocksF32>(sc, cam, hdr, err, queue, ctr, st);
+    if (sc.precision == 2) return launch_typed<double, 1>(sc, cam, schedule, hdr, err, queue, ctr, bx, by, st);
+    if (sc.mode == 1) return launch_typed<float, 1>(sc, cam, schedule, hdr, err, queue, ctr, bx, by, st);
+    return launch_typed<float, 0>(sc, cam, schedule, hdr, err, queue, ctr, bx, by, st);
 }
 
 int wavefront_grid(int precision, int device) {
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    cudaError_t e = precision == 2
-        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_wavefront_kernel<double, false, kMinBlocksF64>, kWavefrontBlock, 0)
-        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_wavefront_kernel<float, false, kMinBlocksF32>, kWavefrontBlock, 0);
-    if (e != cudaSuccess) return 0;
+    const void* fn = precision == 2 ? wave_fn<double, 1, false>() : wave_fn<float, 0, false>();
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWavefrontBlock, 0) != cudaSuccess) return 0;
     return sms * per_sm;
 }
 

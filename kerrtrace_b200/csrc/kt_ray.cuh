@@ -61,10 +61,11 @@ struct Tally {
 // Camera ray of sample `sample` of pixel (px, py) (cuda/kernel.cu:108-121): PCG jitter inside
 // the pixel, vertical field of view, aspect on u.  Stated-physics mode with one sample uses the
 // pixel centre.
+template <int MODE>
 __device__ __forceinline__ void pixel_ray(int px, int py, int sample, const Scene& sc,
                                           const Camera& cam, float dir[3]) {
     float jx, jy;
-    if (sc.mode == 1 && sc.spp == 1) {
+    if (MODE == 1 && sc.spp == 1) {
         jx = 0.5f;
         jy = 0.5f;
     } else {
@@ -131,7 +132,7 @@ __device__ __forceinline__ bool ray_start(RayRun<R>& ry, const Camera& cam, cons
 
 // Tolerance of the step starting at s (cuda/kerr_trace.cuh:67-73): scaled by the Kerr-Schild
 // potential from 5x far away down to 0 at Hk >= 0.3 (reference), or down to 1x (stated physics).
-template <class R>
+template <class R, int MODE>
 __device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
     using O = Ops<R>;
     const R aa = sc_aa<R>(sc), M = sc_M<R>(sc);
@@ -142,7 +143,7 @@ __device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
     R t = O::fdiv(Hk - lit<R>(0.05f, 0.05), lit<R>(0.3f, 0.3) - lit<R>(0.05f, 0.05));
     t = O::minr(O::maxr(t, R(0)), R(1));
     const R base = sc_tol<R>(sc);
-    if (sc.mode == 0) return base * (R(5) - R(5) * t);
+    if (MODE == 0) return base * (R(5) - R(5) * t);
     return base * (R(5) - R(4) * t);
 }
 
@@ -185,7 +186,7 @@ __device__ __forceinline__ R crossing_root(R y0, R y1, R k1, R k3, R k4, R k5, R
 // Disk-plane crossing between prev and cur (cuda/kerr_trace.cuh:138-228): hit point on the
 // dense output, Novikov-Thorne disk test, redshift g, temperature from the disk LUT (with FBM
 // modulation), blackbody colour and alpha compositing.
-template <class R>
+template <class R, int MODE>
 __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, const R* k1,
                                                const R* k3, const R* k4, const R* k5,
                                                const R* k6, const R* k7, R h, const Scene& sc,
@@ -196,7 +197,7 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
     const R dy = y0 - y1;
     R t = dy != R(0) ? O::fdiv(y0, dy) : R(0.5);
     t = O::minr(O::maxr(t, R(0)), R(1));
-    if (sc.mode == 1) t = crossing_root<R>(y0, y1, k1[1], k3[1], k4[1], k5[1], k6[1], k7[1], h, t);
+    if (MODE == 1) t = crossing_root<R>(y0, y1, k1[1], k3[1], k4[1], k5[1], k6[1], k7[1], h, t);
     R hit[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c)
@@ -226,7 +227,7 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
     const R u = span > R(0) ? (rh - r_in) / span : R(0);
     R sampled;
     if constexpr (sizeof(R) == 4) {
-        if (sc.mode == 0) sampled = tex1D<float>(sc.disk_tex, u);
+        if (MODE == 0) sampled = tex1D<float>(sc.disk_tex, u);
         else sampled = lut_lerp1<float>(sc.disk_lut, sc.lut_size, u);
     } else {
         sampled = lut_lerp1<double>(sc.disk_lut, sc.lut_size, u);
@@ -242,40 +243,50 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
         const R r3 = rh * rh * rh;
         const R om = R(1) / (a + O::sqrt_rn(r3 * inv_M));
         R phase = phi + (R)sc.noise_winding * om;
-        if (sc.mode == 1) phase += (R)sc.noise_phase;
+        if (MODE == 1) phase += (R)sc.noise_phase;
         R sp, cp;
         O::sincosr(phase, &sp, &cp);
         const R nu = rh * cp * (R)sc.noise_scale;
         const R nv = rh * sp * (R)sc.noise_scale;
-        const float nval = fbm2((float)nu, (float)nv, sc.noise_detail, sc.mode == 1 ? sc.noise_seed : 0u);
-        const float modulator = 1.0f + sc.noise_strength * (nval - 0.5f);
-        T *= (R)modulator;
+        const R nval = fbm2<R>(nu, nv, sc.noise_detail, MODE == 1 ? sc.noise_seed : 0u);
+        const R modulator = R(1) + (R)sc.noise_strength * (nval - R(0.5));
+        T *= modulator;
     }
     if (O::isfiniter(T) && T > R(0)) {
-        float3 c;
-        if constexpr (sizeof(R) == 4) c = blackbody_rgb(T, sc, err);
-        else c = blackbody_rgb_d(T, sc, err);
-        const float luma = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
-        const float luma_s = (float)((double)luma / sc.wl_step);
-        const float alpha = 1.0f - __expf(-luma_s * 0.5f);
-        ry.col[0] += c.x * alpha * ry.tau;
-        ry.col[1] += c.y * alpha * ry.tau;
-        ry.col[2] += c.z * alpha * ry.tau;
-        ry.tau *= (1.0f - alpha);
+        if constexpr (sizeof(R) == 4) {
+            const float3 c = blackbody_rgb<MODE>(T, sc, err);
+            const float luma = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+            const float luma_s = (float)((double)luma / sc.wl_step);
+            const float alpha = 1.0f - __expf(-luma_s * 0.5f);
+            ry.col[0] += c.x * alpha * ry.tau;
+            ry.col[1] += c.y * alpha * ry.tau;
+            ry.col[2] += c.z * alpha * ry.tau;
+            ry.tau *= (1.0f - alpha);
+        } else {
+            const float3 c = blackbody_rgb_d(T, sc, err);
+            const double luma = 0.2126 * (double)c.x + 0.7152 * (double)c.y + 0.0722 * (double)c.z;
+            const double luma_s = luma / sc.wl_step;
+            const double alpha = 1.0 - exp(-luma_s * 0.5);
+            ry.col[0] += (float)((double)c.x * alpha * (double)ry.tau);
+            ry.col[1] += (float)((double)c.y * alpha * (double)ry.tau);
+            ry.col[2] += (float)((double)c.z * alpha * (double)ry.tau);
+            ry.tau *= (float)(1.0 - alpha);
+        }
     }
 }
 
 // One DP5(4) attempt; on the last attempt of a step, the commit and the per-step tests.
 // Returns true when the ray has finished (its colour is final).
-template <class R, bool COUNT>
+template <class R, int MODE, bool COUNT>
 __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint32_t* err,
                                             Tally& tl) {
+    constexpr bool EXACT = MODE == 1;
     using O = Ops<R>;
     using C = DP<R>;
     const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
-    if (ry.attempt == 0) ry.tol = step_tolerance<R>(ry.s, sc);
+    if (ry.attempt == 0) ry.tol = step_tolerance<R, MODE>(ry.s, sc);
     if (!ry.have_k1) {
-        hamilton_rhs<R>(ry.s, ry.pt, a, aa, M, ry.k1);
+        hamilton_rhs<R, EXACT>(ry.s, ry.pt, a, aa, M, ry.k1);
         ry.have_k1 = true;
         if (COUNT) tl.rhs++;
     }
@@ -285,28 +296,28 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     R y[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], nx[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) y[c] = s[c] + h * C::a21 * k1[c];
-    hamilton_rhs<R>(y, ry.pt, a, aa, M, k2);
+    hamilton_rhs<R, EXACT>(y, ry.pt, a, aa, M, k2);
 #pragma unroll
     for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a31 * k1[c] + C::a32 * k2[c]);
-    hamilton_rhs<R>(y, ry.pt, a, aa, M, k3);
+    hamilton_rhs<R, EXACT>(y, ry.pt, a, aa, M, k3);
 #pragma unroll
     for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a41 * k1[c] + C::a42 * k2[c] + C::a43 * k3[c]);
-    hamilton_rhs<R>(y, ry.pt, a, aa, M, k4);
+    hamilton_rhs<R, EXACT>(y, ry.pt, a, aa, M, k4);
 #pragma unroll
     for (int c = 0; c < 6; ++c)
         y[c] = s[c] + h * (C::a51 * k1[c] + C::a52 * k2[c] + C::a53 * k3[c] + C::a54 * k4[c]);
-    hamilton_rhs<R>(y, ry.pt, a, aa, M, k5);
+    hamilton_rhs<R, EXACT>(y, ry.pt, a, aa, M, k5);
 #pragma unroll
     for (int c = 0; c < 6; ++c)
         y[c] = s[c] + h * (C::a61 * k1[c] + C::a62 * k2[c] + C::a63 * k3[c] + C::a64 * k4[c] +
                            C::a65 * k5[c]);
-    hamilton_rhs<R>(y, ry.pt, a, aa, M, k6);
+    hamilton_rhs<R, EXACT>(y, ry.pt, a, aa, M, k6);
     // 5th-order solution; its stage-7 input is the same expression (a7j = b_j), so k7 is FSAL
 #pragma unroll
     for (int c = 0; c < 6; ++c)
         nx[c] = s[c] + h * (C::b1 * k1[c] + C::b3 * k3[c] + C::b4 * k4[c] + C::b5 * k5[c] +
                             C::b6 * k6[c]);
-    hamilton_rhs<R>(nx, ry.pt, a, aa, M, k7);
+    hamilton_rhs<R, EXACT>(nx, ry.pt, a, aa, M, k7);
     // max-norm of the embedded error, per-component scale tol * max(|y_i|, 1)
     R e[6];
 #pragma unroll
@@ -341,7 +352,7 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     const R r_now = ks_radius<R>(ry.s[0], ry.s[1], ry.s[2], aa);
     if (inside_horizon<R>(r_now, sc)) return true;
     if ((prev[1] < R(0) && ry.s[1] >= R(0)) || (prev[1] > R(0) && ry.s[1] <= R(0)))
-        shade_crossing<R>(ry, prev, ry.k1, k3, k4, k5, k6, k7, h, sc, err);
+        shade_crossing<R, MODE>(ry, prev, ry.k1, k3, k4, k5, k6, k7, h, sc, err);
     if (ok) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) ry.k1[c] = k7[c];
@@ -351,11 +362,10 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     }
     if (beyond_escape<R>(r_now, sc)) {
         R ke[6];
-        hamilton_rhs<R>(ry.s, ry.pt, a, aa, M, ke);
+        hamilton_rhs<R, EXACT>(ry.s, ry.pt, a, aa, M, ke);
         if (COUNT) tl.rhs++;
         const R inv = O::rsq(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
-        const float sky = sky_value((float)(ke[0] * inv), (float)(ke[1] * inv), (float)(ke[2] * inv),
-                                    ry.tau, sc);
+        const float sky = sky_value<R>(ke[0] * inv, ke[1] * inv, ke[2] * inv, ry.tau, sc);
         ry.col[0] += sky;
         ry.col[1] += sky;
         ry.col[2] += sky;

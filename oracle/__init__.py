@@ -81,6 +81,7 @@ def olib() -> C.CDLL:
         L.kto_ks_radius.argtypes = [C.c_double] * 4
         L.kto_ks_radius.restype = C.c_double
         L.kto_rhs.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p]
+        L.kto_rhs_reference.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p]
         L.kto_dense.argtypes = [C.c_void_p, C.c_double]
         L.kto_dense.restype = C.c_double
         L.kto_dense_slope.argtypes = [C.c_void_p, C.c_double]
@@ -91,7 +92,9 @@ def olib() -> C.CDLL:
         L.kto_aces.restype = C.c_double
         L.kto_srgb.argtypes = [C.c_double]
         L.kto_srgb.restype = C.c_double
-        L.kto_dp5_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+        L.kto_dp5_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
+        L.kto_null_init.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
         _olib = L
     return _olib
 

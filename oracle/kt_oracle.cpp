@@ -150,7 +150,9 @@ template <class T> T ks_radius(T x, T y, T z, T aa) {
 }
 
 // dx/dl = p - 2 Hk (l.p - pt) l ;  dp/dl = grad(Hk) (l.p - pt)^2 + 2 Hk (l.p - pt) grad(l).p
-template <class T> void hamilton_rhs(const T* st, T pt, T a, T aa, T Mm, T* d) {
+// exact = false reproduces the reference's d(r^2)/dy = y (1 + (u + 4a^2)/(2s)) (kerr_math.cuh:97);
+// exact = true uses the derivative of r^2 = (u + s)/2, y (1 + (u + 2a^2)/s).
+template <class T> void hamilton_rhs(const T* st, T pt, T a, T aa, T Mm, T* d, bool exact) {
     using F = M<T>;
     const T x = st[0], y = st[1], z = st[2], px = st[3], py = st[4], pz = st[5];
     const T rho2 = x * x + y * y + z * z;
@@ -160,7 +162,7 @@ template <class T> void hamilton_rhs(const T* st, T pt, T a, T aa, T Mm, T* d) {
     const T r = F::sqrt_(r2);
     // r^4 - (rho^2 - a^2) r^2 - a^2 y^2 = 0  =>  d(r^2)/dx_i
     const T dr2x = x * (T(1) + u / s);
-    const T dr2y = y * (T(1) + (u + T(4) * aa) / (T(2) * s));
+    const T dr2y = exact ? y * (T(1) + (u + T(2) * aa) / s) : y * (T(1) + (u + T(4) * aa) / (T(2) * s));
     const T dr2z = z * (T(1) + u / s);
     const T rx = dr2x / (T(2) * r), ry = dr2y / (T(2) * r), rz = dr2z / (T(2) * r);
     const T D = r2 + aa;
@@ -393,7 +395,7 @@ RayResult trace_ray(const kto_scene& s, const Derived& dv, const float dirf[3], 
             while (!accepted && att < s.max_attempts) {
                 hs = h;
                 if (!k1_ready) {
-                    hamilton_rhs<T>(st, pt, a, aa, Mm, k[0]);
+                    hamilton_rhs<T>(st, pt, a, aa, Mm, k[0], s.mode == 1);
                     info.rhs++;
                     k1_ready = true;
                 }
@@ -409,11 +411,11 @@ RayResult trace_ray(const kto_scene& s, const Derived& dv, const float dirf[3], 
                         for (int l = 0; l < j; ++l) acc += A[j - 1][l] * k[l][c];
                         y[c] = st[c] + hs * acc;
                     }
-                    hamilton_rhs<T>(y, pt, a, aa, Mm, k[j]);
+                    hamilton_rhs<T>(y, pt, a, aa, Mm, k[j], s.mode == 1);
                 }
                 for (int c = 0; c < 6; ++c)
                     nx[c] = st[c] + hs * (C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] + C::b6 * k[5][c]);
-                hamilton_rhs<T>(nx, pt, a, aa, Mm, k[6]);
+                hamilton_rhs<T>(nx, pt, a, aa, Mm, k[6], s.mode == 1);
                 info.rhs += 6;
                 errv = T(0);
                 bool all_nan = true;
@@ -540,7 +542,7 @@ RayResult trace_ray(const kto_scene& s, const Derived& dv, const float dirf[3], 
             }
             if ((double)r_now > dv.escape) {
                 T ke[6];
-                hamilton_rhs<T>(st, pt, a, aa, Mm, ke);
+                hamilton_rhs<T>(st, pt, a, aa, Mm, ke, s.mode == 1);
                 info.rhs++;
                 const T nrm = F::sqrt_(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
                 const T ex = ke[0] / nrm, ey = ke[1] / nrm, ez = ke[2] / nrm;
@@ -772,20 +774,44 @@ uint32_t kto_pcg32(uint64_t state) { return pcg32(state); }
 
 // Scalar kernels in f64 for known-answer tests.
 double kto_ks_radius(double x, double y, double z, double a) { return ks_radius<double>(x, y, z, a * a); }
-void kto_rhs(const double* st, double pt, double a, double mass, double* d) { hamilton_rhs<double>(st, pt, a, a * a, mass, d); }
+void kto_rhs(const double* st, double pt, double a, double mass, double* d) { hamilton_rhs<double>(st, pt, a, a * a, mass, d, true); }
+void kto_rhs_reference(const double* st, double pt, double a, double mass, double* d) {
+    hamilton_rhs<double>(st, pt, a, a * a, mass, d, false);
+}
 double kto_dense(const double* q, double t) { return dense<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t); }
 double kto_dense_slope(const double* q, double t) { return dense_slope<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t); }
 double kto_fbm(double u, double v, int octaves, uint32_t seed) { return fbm<double>(u, v, octaves, seed); }
 double kto_aces(double x) { return aces(x); }
 double kto_srgb(double x) { return srgb(x); }
 
+// Null initialisation in f64 (kerr_trace.cuh:14-46): state (x, p) and p_t of a photon leaving
+// `cam` along `dir` (normalised here).
+void kto_null_init(const double* cam, const double* dir, double a, double mass, double* st, double* pt_out) {
+    const double aa = a * a;
+    const double dl = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    const double n[3] = {dir[0] / dl, dir[1] / dl, dir[2] / dl};
+    const double x = cam[0], y = cam[1], z = cam[2];
+    const double r = ks_radius<double>(x, y, z, aa), r2 = r * r, D = r2 + aa;
+    const double l[3] = {(r * x - a * z) / D, y / r, (r * z + a * x) / D};
+    const double Hk = mass * r2 * r / (r2 * r2 + aa * y * y);
+    const double ln = l[0] * n[0] + l[1] * n[1] + l[2] * n[2];
+    const double gtt = -1 + 2 * Hk, gtn = 2 * Hk * ln, gnn = 1 + 2 * Hk * ln * ln;
+    const double kt = (-gtn - std::sqrt(gtn * gtn - gtt * gnn)) / gtt;
+    *pt_out = gtt * kt + gtn;
+    st[0] = x;
+    st[1] = y;
+    st[2] = z;
+    for (int c = 0; c < 3; ++c) st[3 + c] = n[c] + 2 * Hk * l[c] * (kt + ln);
+}
+
 // One DP5(4) step of size h on the Hamiltonian flow (f64), returning the 5th-order state and
 // the embedded error vector: used by the convergence-order known-answer test.
-void kto_dp5_step(const double* st, double pt, double a, double mass, double h, double* out, double* err) {
+void kto_dp5_step(const double* st, double pt, double a, double mass, double h, double* out, double* err,
+                  double* kout) {
     using C = Tab<double>;
     double k[7][6], y[6];
     const double aa = a * a;
-    hamilton_rhs<double>(st, pt, a, aa, mass, k[0]);
+    hamilton_rhs<double>(st, pt, a, aa, mass, k[0], true);
     static const double A[6][5] = {{C::a21, 0, 0, 0, 0},           {C::a31, C::a32, 0, 0, 0},
                                    {C::a41, C::a42, C::a43, 0, 0}, {C::a51, C::a52, C::a53, C::a54, 0},
                                    {C::a61, C::a62, C::a63, C::a64, C::a65}, {C::b1, 0, C::b3, C::b4, C::b5}};
@@ -796,8 +822,11 @@ void kto_dp5_step(const double* st, double pt, double a, double mass, double h, 
             if (j == 6) acc = C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] + C::b6 * k[5][c];
             y[c] = st[c] + h * acc;
         }
-        hamilton_rhs<double>(y, pt, a, aa, mass, k[j]);
+        hamilton_rhs<double>(y, pt, a, aa, mass, k[j], true);
     }
+    if (kout)
+        for (int j = 0; j < 7; ++j)
+            for (int c = 0; c < 6; ++c) kout[6 * j + c] = k[j][c];
     for (int c = 0; c < 6; ++c) {
         out[c] = st[c] + h * (C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] + C::b6 * k[5][c]);
         err[c] = h * ((C::b1 - C::bh1) * k[0][c] + (C::b3 - C::bh3) * k[2][c] + (C::b4 - C::bh4) * k[3][c] +
