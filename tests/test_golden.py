@@ -17,7 +17,7 @@ import pytest
 
 import oracle
 from kerrtrace_b200 import workloads
-from tests.helpers import edge_mask, pixel_class
+from tests.helpers import edge_mask, pixel_class, sky_flip
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 SIZES = {"t1": None, "t2": None, "c1": (64, 64), "c2": (192, 108)}
@@ -38,15 +38,6 @@ def load(name):
         cfg = workloads.scaled(cfg, *SIZES[name])
     g = np.load(GOLDEN / f"ref_{name}.npz")
     return cfg, cam, g
-
-
-def sky_flip(a, b, sky_unit):
-    """Pixels whose difference is a grey offset (equal in the three channels) of a visible size:
-    a sky-grid line seen by one trajectory and not the other."""
-    d = a - b
-    grey = (np.abs(d[:, 0] - d[:, 1]) <= 1e-3 * np.abs(d[:, 0]) + 1e-9) & \
-           (np.abs(d[:, 1] - d[:, 2]) <= 1e-3 * np.abs(d[:, 1]) + 1e-9)
-    return grey & (np.abs(d[:, 0]) > 1e-4 * sky_unit)
 
 
 @pytest.mark.parametrize("name", list(SIZES))
