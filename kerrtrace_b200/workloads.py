@@ -1,7 +1,7 @@
 """Named scenes: the benchmark configurations and the small parity scenes.
 
 Each function returns ``(KtConfig, KtCamera)``.  Values the benchmark description leaves open
-are fixed here and documented in DESIGN.md ("Workloads").
+(LUT range, exposure, peak temperature, escape radius) are fixed here.
 
   c1   256x256, FOV 30, r_obs 50, inclination 80, a = 0.9, tolerance 1e-8, h0 0.1,
        20000 steps, horizon at 1.01 r_h, escape 1000, disk to 20 M, 256-entry LUTs over

@@ -5,7 +5,7 @@
 // or calls it.
 //
 // It restates the reference's algorithm in plain C++, templated on the arithmetic type:
-//   T = double : the f64 oracle (BASELINE's "FP64 CPU oracle")
+//   T = double : the f64 oracle
 //   T = float  : an f32 emulation with correctly rounded operations in place of the GPU's
 //                approximate intrinsics (rsqrtf, __fdividef, __powf, __expf, __sincosf)
 // Sources followed (reference file:line):
