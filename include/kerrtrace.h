@@ -213,6 +213,34 @@ kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const
  * kt_bloom_horizontal followed by kt_post_process. */
 kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_t* image_out);
 
+/* ---- trace without any device allocation --------------------------------------------------- */
+/* Largest n_views of one kt_trace_noalloc call: its scratch is one 32-bit work counter per view,
+ * held in a 256-byte array inside the library's device image. */
+#define KT_NOALLOC_MAX_VIEWS 64
+/*
+ * No counterpart in the reference.  For callers that cannot allocate device memory where they
+ * render: hosts whose device memory all belongs to their own pool allocator, and per-frame
+ * paths that must not call cudaMalloc/cudaFree because those synchronise the device and stall
+ * the frames in flight.  Such a caller cannot create a kt_context (it allocates LUT textures and
+ * a work counter), so this call takes everything from the caller and allocates nothing:
+ *   cfg        scene configuration (reference semantics, FP32: mode KT_MODE_REF, precision FP32)
+ *   cams       host array of n_views cameras (1 <= n_views <= KT_NOALLOC_MAX_VIEWS, else
+ *              KT_ERR_INVALID_ARG with a message)
+ *   bb_lut     dev float[lut_size*4], the blackbody LUT (kt_generate_blackbody_lut layout)
+ *   disk_lut   dev float[lut_size], the disk temperature LUT (kt_generate_disk_lut)
+ *   hdr_out    dev float[n_views*W*H*4], view v at offset v*W*H*4
+ *   err_words  dev uint32[2*n_views], the LUT error word of each view (not cleared here)
+ * It runs the wavefront tracer on the current device and stream, reading the LUTs through a
+ * model of the texture unit's filter, so its images match kt_trace to the parity tolerance.
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture.  Every call shares the scratch: calls that overlap on the GPU race and must be
+ * serialised by the caller.
+ */
+kt_status kt_trace_noalloc(const kt_config* cfg, const kt_camera* cams, uint32_t n_views,
+                           const float* bb_lut, const float* disk_lut, void* stream,
+                           float* hdr_out, uint32_t* err_words);
+
 /* ---- CudaRenderer mirror (src/renderer/mod.rs:469-687) ------------------------------------ */
 /* CudaRenderer::new (mod.rs:470-511): context + two frame buffers with pinned host images. */
 kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out);

@@ -29,6 +29,7 @@ KT_ERR_TIMEOUT = 8
 MODE_REF, MODE_SPEC = 0, 1
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
 SCHED_PLAIN, SCHED_WAVEFRONT = 0, 1
+NOALLOC_MAX_VIEWS = 64
 
 
 class KtConfig(C.Structure):
@@ -120,6 +121,8 @@ SIGNATURES = [
     ("kt_bloom_horizontal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_post_process", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_post_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_trace_noalloc", C.c_int, [C.POINTER(KtConfig), C.POINTER(KtCamera), C.c_uint32, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_renderer_new", C.c_int, [C.POINTER(KtConfig), C.c_int, C.POINTER(C.c_void_p)]),
     ("kt_renderer_submit_render", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                             C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,

@@ -334,8 +334,37 @@ __device__ __forceinline__ float4 lut_lerp4(const float4* __restrict__ lut, int 
                        (float)(a.z + w * (b.z - a.z)), 0.0f);
 }
 
+// Software model of the texture unit's linear filter for plain device arrays (used where no
+// texture object exists): the same coordinate, the weight rounded to 1/256 as the hardware's
+// 1.8 fixed-point weight (checked against the texture unit to about 2e-5 of the LUT range).
+__device__ __forceinline__ void tex_model_coord(int n, float u, int& i0, int& i1, float& w) {
+    const float x = u * (float)n - 0.5f;
+    const float fl = floorf(x);
+    w = rintf((x - fl) * 256.0f) * (1.0f / 256.0f);
+    const float flc = fminf(fmaxf(fl, -1.0f), (float)(n - 1));
+    i0 = fl == fl ? (int)flc : 0;
+    i1 = min(i0 + 1, n - 1);
+    i0 = max(i0, 0);
+}
+__device__ __forceinline__ float lut_tex_model1(const float* __restrict__ lut, int n, float u) {
+    int i0, i1;
+    float w;
+    tex_model_coord(n, u, i0, i1, w);
+    return (1.0f - w) * __ldg(lut + i0) + w * __ldg(lut + i1);
+}
+__device__ __forceinline__ float4 lut_tex_model4(const float4* __restrict__ lut, int n, float u) {
+    int i0, i1;
+    float w;
+    tex_model_coord(n, u, i0, i1, w);
+    const float4 a = __ldg(lut + i0), b = __ldg(lut + i1);
+    const float v = 1.0f - w;
+    return make_float4(v * a.x + w * b.x, v * a.y + w * b.y, v * a.z + w * b.z, 0.0f);
+}
+
 // Blackbody colour of temperature T with the reference's overflow report
 // (cuda/kernel.cu:1-16): above lut_max_temp the first thread to notice records T.
+// MODE 0 samples the texture object, MODE 2 the plain array through the texture-unit model,
+// MODE 1 the plain array with the exact weight.
 template <int MODE>
 __device__ __forceinline__ float3 blackbody_rgb(float T, const Scene& sc, uint32_t* err) {
     if (T > sc.lut_max_temp) {
@@ -347,6 +376,7 @@ __device__ __forceinline__ float3 blackbody_rgb(float T, const Scene& sc, uint32
     const float u = (pos + 0.5f) / (float)sc.lut_size;
     float4 c;
     if (MODE == 0) c = tex1D<float4>(sc.bb_tex, u);
+    else if (MODE == 2) c = lut_tex_model4(sc.bb_lut, sc.lut_size, u);
     else c = lut_lerp4<float>(sc.bb_lut, sc.lut_size, u);
     return make_float3(c.x, c.y, c.z);
 }

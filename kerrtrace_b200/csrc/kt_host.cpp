@@ -641,6 +641,26 @@ kt_status create_impl(const kt_config* cfg, int device, const float* bb_in, cons
     return KT_OK;
 }
 
+}  // namespace
+
+namespace ktd {
+// Device-side scene constants of a config without a context (the LUT pointers and texture
+// objects are left empty for the caller to fill).
+kt_status scene_from_config(const kt_config* cfg, Scene* out) {
+    kt_status st = validate_cfg(cfg);
+    if (st != KT_OK) return st;
+    kt_context tmp;
+    tmp.cfg = *cfg;
+    if ((st = kt_build_kerr_params(cfg, &tmp.params)) != KT_OK) return st;
+    if ((st = fill_scene(&tmp)) != KT_OK) return st;
+    *out = tmp.scene;
+    return KT_OK;
+}
+kt_status set_error(kt_status s, const char* msg) { return fail(s, "%s", msg); }
+}  // namespace ktd
+
+namespace {
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {

@@ -37,3 +37,10 @@ cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t*
 int wavefront_grid(int precision, int device);
 
 }  // namespace ktd
+
+// Host helpers shared with the allocation-free entry point (kt_noalloc.cu).
+#include "../../include/kerrtrace.h"
+namespace ktd {
+kt_status scene_from_config(const kt_config* cfg, Scene* out);
+kt_status set_error(kt_status s, const char* msg);
+}  // namespace ktd

@@ -8,6 +8,9 @@
 // lanes busy on the expensive part (six RHS evaluations), and a lane whose ray has ended can be
 // refilled with a new ray without waiting for its neighbours.
 //
+// MODE: 0 reference semantics (LUTs through texture objects), 1 stated physics, 2 reference
+// semantics with the LUTs read from plain device arrays through a model of the texture unit.
+//
 // Arithmetic follows the reference expression by expression; the only behavioural addition is
 // retirement of rays whose state has become NaN (see ray_advance), which cannot change the
 // output: once y is NaN every later crossing / horizon / escape comparison is false and the
@@ -143,7 +146,7 @@ __device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
     R t = O::fdiv(Hk - lit<R>(0.05f, 0.05), lit<R>(0.3f, 0.3) - lit<R>(0.05f, 0.05));
     t = O::minr(O::maxr(t, R(0)), R(1));
     const R base = sc_tol<R>(sc);
-    if (MODE == 0) return base * (R(5) - R(5) * t);
+    if (MODE != 1) return base * (R(5) - R(5) * t);
     return base * (R(5) - R(4) * t);
 }
 
@@ -228,6 +231,7 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
     R sampled;
     if constexpr (sizeof(R) == 4) {
         if (MODE == 0) sampled = tex1D<float>(sc.disk_tex, u);
+        else if (MODE == 2) sampled = lut_tex_model1(sc.disk_lut, sc.lut_size, u);
         else sampled = lut_lerp1<float>(sc.disk_lut, sc.lut_size, u);
     } else {
         sampled = lut_lerp1<double>(sc.disk_lut, sc.lut_size, u);

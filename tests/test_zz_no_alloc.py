@@ -1,0 +1,99 @@
+"""kt_trace_noalloc: the trace entry point for callers that cannot allocate device memory where
+they render (their device memory belongs to their own pool allocator, or a per-frame path must
+not call cudaMalloc/cudaFree, which synchronise the device).  The call takes the scene, cameras,
+LUTs and outputs from the caller and keeps its only scratch, one work counter per view, in a
+static array inside the library; this test checks its images against kt_trace, the entry point
+with a context, on two calls in a row, and that sizes beyond the scratch are refused.
+
+Buffers here are allocated by the test (the caller's side of the contract) with torch."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import kerrtrace_b200 as kt
+from kerrtrace_b200 import workloads
+from tests.helpers import compare_hdr
+
+pytestmark = pytest.mark.gpu
+
+
+def _views(cam, n):
+    """n cameras around the hole at the scene's radius and inclination."""
+    r = float(np.linalg.norm(np.array(cam.cam_pos)))
+    incl = float(np.degrees(np.arccos(cam.cam_pos[1] / r)))
+    fov = 2 * float(np.degrees(np.arctan(cam.fov_scale)))
+    return [kt.orbit_camera(r, incl, fov, azimuth_deg=37.0 * v) for v in range(n)]
+
+
+def _noalloc(torch, cfg, cams, bb, disk):
+    """Returns (hdr, err, device bytes freed by the call itself: negative if it allocated)."""
+    n = cfg.width * cfg.height
+    hdr = torch.full((len(cams), n, 4), -1.0, device="cuda")
+    err = torch.zeros((len(cams), 2), dtype=torch.int32, device="cuda")
+    arr = (kt.KtCamera * len(cams))(*cams)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    kt.check(kt.lib().kt_trace_noalloc(C.byref(cfg), arr, len(cams), C.c_void_p(bb.data_ptr()),
+                                       C.c_void_p(disk.data_ptr()), None, C.c_void_p(hdr.data_ptr()),
+                                       C.c_void_p(err.data_ptr())))
+    torch.cuda.synchronize()
+    delta = torch.cuda.mem_get_info()[0] - free_before
+    return hdr.cpu().numpy(), err.cpu().numpy().view(np.uint32), delta
+
+
+def _with_context(torch, ctx, cfg, cam):
+    n = cfg.width * cfg.height
+    hdr = torch.zeros((n, 4), device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), 0, kt.SCHED_WAVEFRONT)
+    torch.cuda.synchronize()
+    return hdr.cpu().numpy(), err.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("name,size", [("t1", None), ("c2", (256, 144))])
+def test_noalloc_matches_context_entry_point(cuda, name, size):
+    cfg, cam = workloads.scene(name)
+    if size:
+        cfg = workloads.scaled(cfg, *size)
+    p = kt.build_kerr_params(cfg)
+    bb = cuda.from_numpy(kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start,
+                                                   cfg.wavelength_end, cfg.wavelength_step)).cuda()
+    disk = cuda.from_numpy(kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)).cuda()
+    ctx = kt.Context(cfg)
+    cams = _views(cam, 3)
+    expected = [_with_context(cuda, ctx, cfg, c) for c in cams]
+    # two calls in a row: 3 views, then 2 views (the scratch keeps the previous call's counters)
+    for call, views in enumerate((cams, cams[1:])):
+        hdr, err, delta = _noalloc(cuda, cfg, views, bb, disk)
+        if call == 1:
+            assert delta >= 0  # the call took no device memory (the first call may load the module)
+        for v, c in enumerate(views):
+            exp_hdr, exp_err = expected[cams.index(c)]
+            r = compare_hdr(hdr[v], exp_hdr, cfg.width, cfg.height)
+            assert r["class_mismatch_inner"] == 0, (call, v, r)
+            assert r["over_tol_inner"] == 0, (call, v, r)
+            assert r["over_tol_all"] <= max(2, 0.005 * r["n"]), (call, v, r)
+            assert np.array_equal(err[v], exp_err)
+            assert np.all(hdr[v][:, 3] == 1.0)  # every pixel written
+    ctx.close()
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
+    cfg, cam = workloads.scene("t2")
+    dummy = cuda.zeros(16, device="cuda")
+    for n in (0, kt.NOALLOC_MAX_VIEWS + 1):
+        arr = (kt.KtCamera * max(n, 1))(*([cam] * max(n, 1)))
+        st = kt.lib().kt_trace_noalloc(C.byref(cfg), arr, n, C.c_void_p(dummy.data_ptr()),
+                                       C.c_void_p(dummy.data_ptr()), None, C.c_void_p(dummy.data_ptr()),
+                                       C.c_void_p(dummy.data_ptr()))
+        assert st == kt.KT_ERR_INVALID_ARG
+        assert "views" in kt.lib().kt_last_error().decode()
+    c = cfg.copy()
+    c.mode = kt.MODE_SPEC
+    arr = (kt.KtCamera * 1)(cam)
+    st = kt.lib().kt_trace_noalloc(C.byref(c), arr, 1, C.c_void_p(dummy.data_ptr()), C.c_void_p(dummy.data_ptr()),
+                                   None, C.c_void_p(dummy.data_ptr()), C.c_void_p(dummy.data_ptr()))
+    assert st == kt.KT_ERR_UNSUPPORTED
