@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2")
-    ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "plain"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "wavefront", "plain"])
+    ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--size", default=None, help="WxH override of the scene resolution (same scene otherwise)")
@@ -190,14 +191,67 @@ def cpu_baseline(cfg, cam, budget_s: float) -> dict:
     return {"value": round(rays / t / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample}
 
 
+def precision_leg(cfg, cam, local, reps: int) -> dict:
+    """Stated-physics traces of the same frame in FP32, mixed precision and FP64: Mrays/s of
+    each (trace kernel, event-timed, autotuned launch shape) and the per-pixel error of FP32 and
+    mixed against the FP64 run (HDR RGB, and radius / redshift of the first disk hit)."""
+    import numpy as np
+    import torch
+
+    import kerrtrace_b200 as kt
+    from kerrtrace_b200 import autotune
+
+    n = cfg.width * cfg.height
+    hdr = torch.zeros((n, 4), device="cuda")
+    aux = torch.zeros((n, 4), device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    out, runs = {}, {}
+    for name, prec in (("fp64", kt.PREC_FP64), ("fp32", kt.PREC_FP32), ("mixed", kt.PREC_MIXED)):
+        c = cfg.copy()
+        c.mode, c.precision = kt.MODE_SPEC, prec
+        ctx = kt.Context(c, local)
+        tuned = autotune.autotune(ctx, cam, reps=2, stream=stream)
+        st = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO, aux.data_ptr())
+        out[name] = (hdr.cpu().numpy()[:, :3].astype(np.float64), aux.cpu().numpy().astype(np.float64))
+        ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+        torch.cuda.synchronize()
+        k = max(1, reps if prec != kt.PREC_FP64 else reps // 3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / k
+        runs[name] = {"mrays_s": round(n * cfg.spp / ms / 1e3, 2), "trace_ms": round(ms, 4), "steps": int(st.steps),
+                      "fp64_zone_steps": int(st.fp64_steps), "tuning": tuned.best}
+        ctx.close()
+    ref, ref_aux = out["fp64"]
+    floor = 1e-6 * np.abs(ref).max()
+    for name in ("fp32", "mixed"):
+        a, a_aux = out[name]
+        rel = (np.abs(a - ref) / np.maximum(np.abs(ref), floor)).max(1)
+        hit = np.isfinite(a_aux[:, 0]) & np.isfinite(ref_aux[:, 0])
+        rr = np.abs(a_aux[hit, 0] - ref_aux[hit, 0]) / np.abs(ref_aux[hit, 0])
+        rg = np.abs(a_aux[hit, 1] - ref_aux[hit, 1]) / np.abs(ref_aux[hit, 1])
+        runs[name]["err_vs_fp64"] = {
+            "hdr_p99": float(np.quantile(rel, 0.99)), "hdr_p999": float(np.quantile(rel, 0.999)),
+            "hdr_frac_over_1e-3": float(np.mean(rel > 1e-3)),
+            "r_cross_p99": float(np.quantile(rr, 0.99)) if hit.any() else None,
+            "g_p99": float(np.quantile(rg, 0.99)) if hit.any() else None,
+            "hit_class_mismatch": int(np.sum(np.isfinite(a_aux[:, 0]) != np.isfinite(ref_aux[:, 0])))}
+    return runs
+
+
 def run_ours(args, rank, world, local):
     import torch
 
     import kerrtrace_b200 as kt
-    from kerrtrace_b200 import flops, workloads
+    from kerrtrace_b200 import autotune, flops, workloads
 
     cfg, cam = rank_camera(kt, workloads, args.workload, rank, world, args.size)
-    sched = kt.SCHED_WAVEFRONT if args.schedule == "wavefront" else kt.SCHED_PLAIN
+    sched = {"auto": kt.SCHED_AUTO, "wavefront": kt.SCHED_WAVEFRONT, "plain": kt.SCHED_PLAIN}[args.schedule]
     ctx = kt.Context(cfg, local)
     n = cfg.width * cfg.height
     hdr = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
@@ -206,6 +260,7 @@ def run_ours(args, rank, world, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
 
+    tuned = autotune.autotune(ctx, cam, stream=stream) if sched == kt.SCHED_AUTO else None
     stats = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), stream, sched)
     work = flops.trace_flops(stats)
 
@@ -240,9 +295,10 @@ def run_ours(args, rank, world, local):
     rays_all = n * cfg.spp * world * args.steps
     value = rays_all / (total_ms / 1e3) / 1e6
 
-    # end to end through the renderer API (host buffers)
+    # end to end through the renderer API (host buffers), same launch shape
     rend = kt.Renderer(cfg, local)
     rend.set_schedule(sched)
+    rend.set_tuning(ctx.tuning())
     cam_args = (list(cam.cam_pos), list(cam.fwd), list(cam.rgt), list(cam.up), cam.fov_scale)
 
     def frame():
@@ -261,20 +317,23 @@ def run_ours(args, rank, world, local):
         frame()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     rend.close()
-    e2e = {"value": rays_all / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 52,
-           "d2h_bytes_per_step": n * 4 + 8, "ms_per_step": e2e_s * 1e3 / args.steps}
+    e2e = {"value": round(rays_all / e2e_s / 1e6, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 52,
+           "d2h_bytes_per_step": n * 4 + 8, "ms_per_step": round(e2e_s * 1e3 / args.steps, 4)}
 
     trace_ms = sum(t_trace) / len(t_trace)
     achieved = work / (trace_ms / 1e3) / 1e12
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     mhz = clocks.get("sm_mhz") or 1965.0
     peak = sms * flops.FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
-    roofline = {"bound": "fp32", "kernel": "trace_wavefront_kernel" if sched else "trace_plain_kernel",
+    t = ctx.tuning()
+    kernel = "trace_plain_kernel" if (t.schedule == kt.SCHED_PLAIN and sched == kt.SCHED_AUTO) or sched == kt.SCHED_PLAIN \
+        else "trace_wavefront_kernel"
+    roofline = {"bound": "fp32", "kernel": kernel,
                 "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4),
                 "peak_source": f"FP32 FMA peak at the sampled median SM clock ({mhz:.0f} MHz): "
                                f"{sms} SMs x 128 lanes x 2 flops",
-                "traffic": TRACE_TRAFFIC_PER_RAY * n * cfg.spp,
+                "traffic": int(TRACE_TRAFFIC_PER_RAY * n * cfg.spp),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one trace launch "
                                   "(c2 scene at 960x540: 156928 + 0 B), scaled to this launch by its rays",
                 "trace_ms": round(trace_ms, 4),
@@ -289,11 +348,16 @@ def run_ours(args, rank, world, local):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, camera rays)",
         "config": {"workload": f"{args.workload}: {cfg.width}x{cfg.height}, a={cfg.spin:.3f}, tol={cfg.tolerance:g}, "
                                f"max_steps={cfg.max_steps}, spp={cfg.spp}, bloom r={cfg.bloom_radius:g}",
-                   "schedule": args.schedule, "mode": "reference semantics (drop-in)", "precision": "fp32",
-                   "l2": "flushed between steps (256 MiB write outside the timed events)",
+                   "schedule": args.schedule, "tuning": t.as_dict(),
+                   "mode": "reference semantics (drop-in, bit-identical to the reference kernel)",
+                   "precision": "fp32", "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"replica frames x{world}"},
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": 2 * args.steps,
     }
+    if tuned is not None:
+        line["autotune"] = tuned.summary()
+    if rank == 0 and world == 1 and not args.no_precision:
+        line["precision"] = precision_leg(cfg, cam, local, max(3, args.steps))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, cam, args.cpu_seconds)
     if rank == 0:

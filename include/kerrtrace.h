@@ -57,11 +57,21 @@ typedef enum kt_mode { KT_MODE_REF = 0, KT_MODE_SPEC = 1 } kt_mode;
  * solve.  FP64 runs the whole integration in double. */
 typedef enum kt_precision { KT_PREC_FP32 = 0, KT_PREC_MIXED = 1, KT_PREC_FP64 = 2 } kt_precision;
 
-/* Scheduling of the trace kernel. */
+/* Scheduling of the trace kernel.  All schedules produce the same image bits. */
 typedef enum kt_schedule {
     KT_SCHED_PLAIN = 0,     /* one thread per pixel on a 2D grid of block_dim tiles (kernel.cu:88) */
-    KT_SCHED_WAVEFRONT = 1  /* persistent kernel, per-lane refill from a device work queue */
+    KT_SCHED_WAVEFRONT = 1, /* persistent kernel, lanes refilled from a device work counter */
+    KT_SCHED_AUTO = 2       /* whichever the context's kt_tuning selects (the autotuner's choice) */
 } kt_schedule;
+
+/* Launch shape used by KT_SCHED_AUTO (see kt_context_set_tuning). */
+typedef struct kt_tuning {
+    int32_t schedule;      /* KT_SCHED_PLAIN or KT_SCHED_WAVEFRONT */
+    int32_t block_x;       /* plain: block shape, 0 = the config's block_dim */
+    int32_t block_y;
+    int32_t blocks_per_sm; /* wavefront: resident blocks of 128 threads per SM, 3..6 */
+    int32_t refill_min;    /* wavefront: idle lanes a warp collects before refilling them, 1..32 */
+} kt_tuning;
 
 /*
  * Full configuration.  Field names follow the reference's config.yaml / serde structs
@@ -199,10 +209,21 @@ kt_status kt_context_params(const kt_context* ctx, kt_kerr_params* out);
  * which clears it with memset_zeros before the launch, mod.rs:544-546). */
 kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
                    float* hdr_out, uint32_t* err_word);
-/* Same as kt_trace, plus per-launch counters (synchronises the stream to read them). */
+/* Same as kt_trace, plus per-launch counters (synchronises the stream to read them).
+ * aux_out (dev float[4*W*H], may be NULL) receives, per pixel, the first shaded disk hit of
+ * sample 0: Kerr-Schild radius, redshift g, temperature T and the number of shaded hits
+ * (NaN where the ray shaded nothing). */
 kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam,
                            int32_t schedule, float* hdr_out, uint32_t* err_word,
-                           kt_trace_stats* stats);
+                           kt_trace_stats* stats, float* aux_out);
+/* Launch shape of the trace (the autotuner's knobs, kerrtrace_b200/autotune.py).  For the
+ * persistent schedule: resident blocks of 128 threads per SM (3..6; the compiler caps registers
+ * per thread accordingly; only the FP32 reference-semantics kernel has the 3/5/6 variants) and
+ * the refill threshold.  For the plain schedule: the block shape (at most 1024 threads).
+ * kt_trace(KT_SCHED_AUTO) runs tuning->schedule; the explicit schedules use the rest of the
+ * tuning too.  Default: wavefront, config block_dim, 4 blocks per SM, refill 1. */
+kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* tuning);
+kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* tuning);
 /* bloom_horizontal (cuda/kernel.cu:144-173): dev float4 hdr -> dev float4 bloom. */
 kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom);
 /* post_process (cuda/kernel.cu:175-251): vertical blur + composite + ACES + sRGB + pack to
@@ -258,8 +279,10 @@ kt_status kt_renderer_finish_frame(kt_renderer* r, uint32_t index);
 /* Blocks until every submitted frame is complete (no reference counterpart; used by hosts
  * that render headless). */
 kt_status kt_renderer_wait(kt_renderer* r);
-/* Selects the trace schedule used by submit_render (default KT_SCHED_WAVEFRONT). */
+/* Selects the trace schedule used by submit_render (default KT_SCHED_AUTO). */
 kt_status kt_renderer_set_schedule(kt_renderer* r, int32_t schedule);
+/* Sets the launch shape of the renderer's context (kt_context_set_tuning). */
+kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning);
 /* The device HDR buffer of a frame (valid until the frame is resubmitted). */
 kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev);
 void kt_renderer_destroy(kt_renderer* r);

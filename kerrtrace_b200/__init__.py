@@ -28,7 +28,7 @@ KT_ERR_TIMEOUT = 8
 
 MODE_REF, MODE_SPEC = 0, 1
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
-SCHED_PLAIN, SCHED_WAVEFRONT = 0, 1
+SCHED_PLAIN, SCHED_WAVEFRONT, SCHED_AUTO = 0, 1, 2
 NOALLOC_MAX_VIEWS = 64
 
 
@@ -86,6 +86,16 @@ class KtTraceStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("rays", "steps", "attempts", "rhs_evals", "frozen_rays", "fp64_steps")]
 
 
+class KtTuning(C.Structure):
+    """Mirror of ``kt_tuning``: the launch shape that KT_SCHED_AUTO runs."""
+
+    _fields_ = [("schedule", C.c_int32), ("block_x", C.c_int32), ("block_y", C.c_int32),
+                ("blocks_per_sm", C.c_int32), ("refill_min", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class KtError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"kerrtrace status {status}: {message}")
@@ -117,7 +127,10 @@ SIGNATURES = [
     ("kt_context_params", C.c_int, [C.c_void_p, C.POINTER(KtKerrParams)]),
     ("kt_trace", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p]),
     ("kt_trace_counted", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p,
-                                   C.POINTER(KtTraceStats)]),
+                                   C.POINTER(KtTraceStats), C.c_void_p]),
+    ("kt_context_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
+    ("kt_context_get_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
+    ("kt_renderer_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
     ("kt_bloom_horizontal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_post_process", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_post_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -257,11 +270,21 @@ class Context:
                              C.c_void_p(err_ptr)))
 
     def trace_counted(self, cam: KtCamera, hdr_ptr: int, err_ptr: int, stream: int = 0,
-                      schedule: int = SCHED_WAVEFRONT) -> KtTraceStats:
+                      schedule: int = SCHED_WAVEFRONT, aux_ptr: int = 0) -> KtTraceStats:
         st = KtTraceStats()
         check(lib().kt_trace_counted(self.handle, C.c_void_p(stream), C.byref(cam), schedule, C.c_void_p(hdr_ptr),
-                                     C.c_void_p(err_ptr), C.byref(st)))
+                                     C.c_void_p(err_ptr), C.byref(st), C.c_void_p(aux_ptr or None)))
         return st
+
+    def set_tuning(self, schedule: int = SCHED_WAVEFRONT, block_x: int = 0, block_y: int = 0,
+                   blocks_per_sm: int = 4, refill_min: int = 1):
+        t = KtTuning(schedule, block_x, block_y, blocks_per_sm, refill_min)
+        check(lib().kt_context_set_tuning(self.handle, C.byref(t)))
+
+    def tuning(self) -> KtTuning:
+        t = KtTuning()
+        check(lib().kt_context_get_tuning(self.handle, C.byref(t)))
+        return t
 
     def bloom_horizontal(self, hdr_ptr: int, bloom_ptr: int, stream: int = 0):
         check(lib().kt_bloom_horizontal(self.handle, C.c_void_p(stream), C.c_void_p(hdr_ptr), C.c_void_p(bloom_ptr)))
@@ -302,6 +325,9 @@ class Renderer:
 
     def set_schedule(self, schedule: int):
         check(lib().kt_renderer_set_schedule(self.handle, schedule))
+
+    def set_tuning(self, tuning: KtTuning):
+        check(lib().kt_renderer_set_tuning(self.handle, C.byref(tuning)))
 
     def submit_render(self, cam_pos, fwd, rgt, up, fov_scale: float) -> bool:
         arr = lambda v: (C.c_float * 3)(*v)  # noqa: E731

@@ -432,6 +432,7 @@ struct kt_context {
     float4* bb_lut_dev = nullptr;
     float* disk_lut_dev = nullptr;
     unsigned* queue = nullptr;              // wavefront work counter (1 word)
+    ktd::Tuning tuning;                     // persistent-tracer launch shape
     unsigned long long* counters = nullptr; // 6 x u64 for the counting launches
     int block_x = 16, block_y = 16;
 };
@@ -544,10 +545,11 @@ kt_status fill_scene(kt_context* c) {
     s.noise_seed = cfg.noise_seed;
     s.noise_phase = cfg.noise_phase;
     const float zf = cfg.photon_zone_factor > 0.0f ? cfg.photon_zone_factor : 1.5f;
-    // prograde equatorial photon orbit r_ph = 2M (1 + cos(2/3 acos(-|a|/M)))
-    const double an = std::fabs((double)p.a_norm);
-    const double rph = 2.0 * s.M_d * (1.0 + std::cos(2.0 / 3.0 * std::acos(-std::fmin(an, 1.0))));
-    s.zone_r = (float)(zf * std::fmax(rph, 3.0 * s.M_d));
+    // retrograde equatorial photon orbit r_ph = 2M (1 + cos(2/3 acos(|a|/M))): 3M for a = 0,
+    // 4M for |a| = M; the prograde orbit lies inside it
+    const double an = std::fmin(std::fabs((double)p.a_norm), 1.0);
+    const double rph = 2.0 * s.M_d * (1.0 + std::cos(2.0 / 3.0 * std::acos(an)));
+    s.zone_r = (float)(zf * rph);
     s.spec_tol_floor = 1.0f;
     s.width = (int)cfg.width;
     s.height = (int)cfg.height;
@@ -670,6 +672,9 @@ struct DeviceGuard {
     ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
 };
 
+int plain_bx(const kt_context* c) { return c->tuning.block_x > 0 ? c->tuning.block_x : c->block_x; }
+int plain_by(const kt_context* c) { return c->tuning.block_y > 0 ? c->tuning.block_y : c->block_y; }
+
 ktd::Camera to_camera(const kt_camera* cam) {
     ktd::Camera c;
     for (int i = 0; i < 3; ++i) {
@@ -701,27 +706,59 @@ kt_status kt_context_params(const kt_context* ctx, kt_kerr_params* out) {
     return KT_OK;
 }
 
+kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* t) {
+    if (!ctx || !t) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (t->schedule != KT_SCHED_PLAIN && t->schedule != KT_SCHED_WAVEFRONT)
+        return fail(KT_ERR_INVALID_ARG, "tuning schedule %d must be plain or wavefront", t->schedule);
+    if (t->blocks_per_sm < 3 || t->blocks_per_sm > 6) return fail(KT_ERR_INVALID_ARG, "blocks_per_sm %d not in 3..6", t->blocks_per_sm);
+    if (t->refill_min < 1 || t->refill_min > 32) return fail(KT_ERR_INVALID_ARG, "refill_min %d not in 1..32", t->refill_min);
+    if (t->block_x < 0 || t->block_y < 0 || (int64_t)t->block_x * t->block_y > 1024 ||
+        ((t->block_x == 0) != (t->block_y == 0)))
+        return fail(KT_ERR_INVALID_ARG, "plain block %dx%d invalid", t->block_x, t->block_y);
+    ctx->tuning.schedule = t->schedule;
+    ctx->tuning.block_x = t->block_x;
+    ctx->tuning.block_y = t->block_y;
+    ctx->tuning.blocks_per_sm = t->blocks_per_sm;
+    ctx->tuning.refill_min = t->refill_min;
+    return KT_OK;
+}
+kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* t) {
+    if (!ctx || !t) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    t->schedule = ctx->tuning.schedule;
+    t->block_x = ctx->tuning.block_x;
+    t->block_y = ctx->tuning.block_y;
+    t->blocks_per_sm = ctx->tuning.blocks_per_sm;
+    t->refill_min = ctx->tuning.refill_min;
+    return KT_OK;
+}
+
 kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
                    float* hdr_out, uint32_t* err_word) {
     if (!ctx || !cam || !hdr_out || !err_word) return fail(KT_ERR_INVALID_ARG, "NULL argument");
-    if (schedule != KT_SCHED_PLAIN && schedule != KT_SCHED_WAVEFRONT) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
+    if (schedule < KT_SCHED_PLAIN || schedule > KT_SCHED_AUTO) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
     DeviceGuard g(ctx->device);
-    const cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), schedule, reinterpret_cast<float4*>(hdr_out),
-                                            err_word, ctx->queue, nullptr, ctx->block_x, ctx->block_y,
-                                            (cudaStream_t)stream);
+    const int sched = schedule == KT_SCHED_AUTO ? ctx->tuning.schedule : schedule;
+    const cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), sched, reinterpret_cast<float4*>(hdr_out),
+                                            err_word, ctx->queue, nullptr, nullptr, ctx->tuning, plain_bx(ctx),
+                                            plain_by(ctx), (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "trace launch");
     return KT_OK;
 }
 
 kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
-                           float* hdr_out, uint32_t* err_word, kt_trace_stats* stats) {
+                           float* hdr_out, uint32_t* err_word, kt_trace_stats* stats, float* aux_out) {
     if (!ctx || !cam || !hdr_out || !err_word || !stats) return fail(KT_ERR_INVALID_ARG, "NULL argument");
-    if (schedule != KT_SCHED_PLAIN && schedule != KT_SCHED_WAVEFRONT) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
+    if (schedule < KT_SCHED_PLAIN || schedule > KT_SCHED_AUTO) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
     DeviceGuard g(ctx->device);
+    const int sched = schedule == KT_SCHED_AUTO ? ctx->tuning.schedule : schedule;
     cudaStream_t st = (cudaStream_t)stream;
     KT_CUDA(cudaMemsetAsync(ctx->counters, 0, 8 * sizeof(unsigned long long), st), "clear counters");
-    cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), schedule, reinterpret_cast<float4*>(hdr_out),
-                                      err_word, ctx->queue, ctx->counters, ctx->block_x, ctx->block_y, st);
+    if (aux_out)  // all-ones words are NaN: pixels without a traced sample 0 stay NaN
+        KT_CUDA(cudaMemsetAsync(aux_out, 0xff, (size_t)ctx->cfg.width * ctx->cfg.height * 4 * sizeof(float), st),
+                "clear aux");
+    cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), sched, reinterpret_cast<float4*>(hdr_out),
+                                      err_word, ctx->queue, ctx->counters, reinterpret_cast<float4*>(aux_out),
+                                      ctx->tuning, plain_bx(ctx), plain_by(ctx), st);
     if (e != cudaSuccess) return cuda_fail(e, "trace launch");
     unsigned long long h[8];
     KT_CUDA(cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, st), "read counters");
@@ -785,7 +822,7 @@ struct kt_renderer {
     kt_frame frames[2];
     std::deque<uint32_t> pending;
     uint32_t next_frame = 0;
-    int schedule = KT_SCHED_WAVEFRONT;
+    int schedule = KT_SCHED_AUTO;
 };
 
 namespace {
@@ -848,9 +885,14 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
 
 kt_status kt_renderer_set_schedule(kt_renderer* r, int32_t schedule) {
     if (!r) return fail(KT_ERR_INVALID_ARG, "renderer is NULL");
-    if (schedule != KT_SCHED_PLAIN && schedule != KT_SCHED_WAVEFRONT) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
+    if (schedule < KT_SCHED_PLAIN || schedule > KT_SCHED_AUTO) return fail(KT_ERR_INVALID_ARG, "unknown schedule %d", schedule);
     r->schedule = schedule;
     return KT_OK;
+}
+
+kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning) {
+    if (!r) return fail(KT_ERR_INVALID_ARG, "renderer is NULL");
+    return kt_context_set_tuning(r->ctx, tuning);
 }
 
 kt_status kt_renderer_submit_render(kt_renderer* r, const float cam_pos[3], const float fwd[3],

@@ -19,12 +19,23 @@ struct PostParams {
     float threshold;
 };
 
+// Tuning of the persistent tracer: resident blocks per SM (3..6 for the FP32 reference
+// kernel; the default otherwise) and the number of idle lanes a warp waits for before it
+// refills them (1..32).
+struct Tuning {
+    int schedule = 1;
+    int block_x = 0, block_y = 0;
+    int blocks_per_sm = 4;
+    int refill_min = 1;
+};
+
 // Trace launch: schedule 0 = plain 2D grid (block bx x by), 1 = persistent wavefront.
-// precision 0 = FP32, 1 = mixed, 2 = FP64.  queue: one zero-initialised device word per launch
-// (reset here on `stream`).  ctr: optional 6 x u64 device counters (counting kernels).
+// precision 0 = FP32, 1 = mixed, 2 = FP64.  queue: one device word, reset here on `stream`.
+// ctr: optional 6 x u64 device counters (selects the counting kernels); aux: optional float4
+// per pixel with the first shaded disk hit (r, g, T, hits) of sample 0 (counting kernels only).
 cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
-                         uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx, int by,
-                         cudaStream_t stream);
+                         uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
+                         const Tuning& tn, int bx, int by, cudaStream_t stream);
 
 cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, float4* bloom,
                                     cudaStream_t stream);
@@ -32,9 +43,6 @@ cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const f
                                 uint32_t* image, cudaStream_t stream);
 cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image,
                               cudaStream_t stream);
-
-// Resident blocks of the wavefront kernel for this scene's precision (occupancy query).
-int wavefront_grid(int precision, int device);
 
 }  // namespace ktd
 

@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "kt_internal.h"
 #include "kt_ray.cuh"
 
@@ -45,38 +47,46 @@ __device__ __forceinline__ void tally_ray(Tally& acc, const Tally& ray) {
     acc.frozen += ray.frozen ? 1u : 0u;
     acc.fp64 += ray.fp64;
 }
+// First shaded disk hit of sample 0 of a pixel (counting kernels, when aux is given).
+__device__ __forceinline__ void write_aux(float4* aux, size_t idx, const Tally& t) {
+    if (aux) aux[idx] = make_float4(t.first_r, t.first_g, t.first_T, (float)t.hits);
+}
 
 // Runs one ray to completion (plain schedule).
 template <class R, int MODE, bool COUNT>
 __device__ __forceinline__ void run_ray(int px, int py, int smp, const Scene& sc, const Camera& cam,
-                                        uint32_t* err, float acc[3], Tally& total) {
+                                        uint32_t* err, float acc[3], Tally& total, float4* aux) {
     float dir[3];
     pixel_ray<MODE>(px, py, smp, sc, cam, dir);
     RayRun<R> ry;
     Tally tl;
     tl.clear();
-    if (ray_start<R>(ry, cam, dir, sc)) {
-        while (!ray_advance<R, MODE, COUNT>(ry, sc, err, tl)) {
+    if (start(ry, cam, dir, sc)) {
+        while (!advance<MODE, COUNT>(ry, sc, err, tl)) {
         }
     }
     acc[0] += ry.col[0];
     acc[1] += ry.col[1];
     acc[2] += ry.col[2];
-    if (COUNT) tally_ray(total, tl);
+    if (COUNT) {
+        tally_ray(total, tl);
+        if (smp == 0) write_aux(aux, (size_t)py * sc.width + px, tl);
+    }
 }
 
 template <class R, int MODE, bool COUNT, int MAXT>
 __global__ void __launch_bounds__(MAXT) trace_plain_kernel(const Scene sc, const Camera cam,
                                                            float4* __restrict__ hdr,
                                                            uint32_t* __restrict__ err,
-                                                           unsigned long long* __restrict__ ctr) {
+                                                           unsigned long long* __restrict__ ctr,
+                                                           float4* __restrict__ aux) {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
     if (px >= sc.width || py >= sc.height) return;
     float acc[3] = {0.0f, 0.0f, 0.0f};
     Tally total;
     total.clear();
-    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total);
+    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total, aux);
     const float fs = sc.final_scale;
     hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
     if (COUNT) add_tally(ctr, (uint64_t)sc.spp, total);
@@ -100,11 +110,16 @@ __device__ __forceinline__ void unit_to_pixel(unsigned u, int W, int H, int& px,
     px = col0 + (int)(rem2 % (unsigned)wt);
 }
 
+// Persistent wavefront tracer.  A lane whose pixel is done takes a new one from the work
+// counter; lanes are refilled together once at least `refill_min` of the warp's lanes are idle
+// (or when the warp has nothing else to do), which trades idle lanes against how often the
+// divergent start-up code runs.
 template <class R, int MODE, bool COUNT, int MINB>
 __global__ void __launch_bounds__(kWavefrontBlock, MINB)
     trace_wavefront_kernel(const Scene sc, const Camera cam, float4* __restrict__ hdr,
                            uint32_t* __restrict__ err, unsigned* __restrict__ queue,
-                           unsigned long long* __restrict__ ctr) {
+                           unsigned long long* __restrict__ ctr, float4* __restrict__ aux,
+                           int refill_min) {
     const int lane = threadIdx.x & 31;
     const unsigned lane_lt = (1u << lane) - 1u;
     const unsigned n_units = (unsigned)sc.width * (unsigned)sc.height;
@@ -121,9 +136,10 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
     while (true) {
         if (open) {
             const unsigned need = __ballot_sync(kFull, !active);
-            if (need) {
+            const int idle = __popc(need);
+            if (idle >= refill_min || (idle > 0 && idle == 32)) {
                 const int leader = __ffs(need) - 1;
-                const unsigned cnt = (unsigned)__popc(need);
+                const unsigned cnt = (unsigned)idle;
                 unsigned base = 0;
                 if (lane == leader) base = atomicAdd(queue, cnt);
                 base = __shfl_sync(kFull, base, leader);
@@ -138,7 +154,7 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
                             float dir[3];
                             pixel_ray<MODE>(px, py, smp, sc, cam, dir);
                             if (COUNT) tl.clear();
-                            if (ray_start<R>(ry, cam, dir, sc)) break;
+                            if (start(ry, cam, dir, sc)) break;
                         }
                         if (smp < sc.spp) {
                             active = true;
@@ -152,17 +168,23 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
                 }
             }
         }
-        if (!__any_sync(kFull, active)) break;
-        if (active && ray_advance<R, MODE, COUNT>(ry, sc, err, tl)) {
+        if (!__any_sync(kFull, active)) {
+            if (!open) break;
+            continue;
+        }
+        if (active && advance<MODE, COUNT>(ry, sc, err, tl)) {
             acc[0] += ry.col[0];
             acc[1] += ry.col[1];
             acc[2] += ry.col[2];
-            if (COUNT) tally_ray(total, tl);
+            if (COUNT) {
+                tally_ray(total, tl);
+                if (smp == 0) write_aux(aux, (size_t)py * sc.width + px, tl);
+            }
             for (++smp; smp < sc.spp; ++smp) {
                 float dir[3];
                 pixel_ray<MODE>(px, py, smp, sc, cam, dir);
                 if (COUNT) tl.clear();
-                if (ray_start<R>(ry, cam, dir, sc)) break;
+                if (start(ry, cam, dir, sc)) break;
             }
             if (smp >= sc.spp) {
                 const float fs = sc.final_scale;
@@ -176,30 +198,29 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
 }
 
 // ---- launch -------------------------------------------------------------------------------
-constexpr int kMinBlocksF32 = 4;   // 512 resident threads/SM -> <= 128 registers per thread
-constexpr int kMinBlocksF64 = 2;
+// Resident blocks per SM requested from the compiler (which caps registers per thread at
+// 65536 / (128 * MINB)): the default per arithmetic type, and the variants the autotuner may
+// pick for the FP32 reference-semantics kernel.
+template <class R> struct WaveDefaults { static constexpr int minb = 4; };
+template <> struct WaveDefaults<double> { static constexpr int minb = 2; };
+template <> struct WaveDefaults<Mixed> { static constexpr int minb = 4; };
 
 template <class R, int MODE, bool COUNT>
 static cudaError_t launch_plain(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
-                                unsigned long long* ctr, int bx, int by, cudaStream_t st) {
+                                unsigned long long* ctr, float4* aux, int bx, int by, cudaStream_t st) {
     const dim3 block(bx, by);
     const dim3 grid((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
     if (bx * by <= 256)
-        trace_plain_kernel<R, MODE, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
+        trace_plain_kernel<R, MODE, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux);
     else
-        trace_plain_kernel<R, MODE, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr);
+        trace_plain_kernel<R, MODE, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux);
     return cudaGetLastError();
 }
 
-template <class R, int MODE, bool COUNT>
-static const void* wave_fn() {
-    return (const void*)trace_wavefront_kernel<R, MODE, COUNT, sizeof(R) == 4 ? kMinBlocksF32 : kMinBlocksF64>;
-}
-
-template <class R, int MODE, bool COUNT>
-static cudaError_t launch_wave(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
-                               unsigned* queue, unsigned long long* ctr, cudaStream_t st) {
-    constexpr int MINB = sizeof(R) == 4 ? kMinBlocksF32 : kMinBlocksF64;
+template <class R, int MODE, bool COUNT, int MINB>
+static cudaError_t launch_wave_minb(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
+                                    unsigned* queue, unsigned long long* ctr, float4* aux, int refill,
+                                    cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -212,36 +233,45 @@ static cudaError_t launch_wave(const Scene& sc, const Camera& cam, float4* hdr, 
     e = cudaMemsetAsync(queue, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
     trace_wavefront_kernel<R, MODE, COUNT, MINB>
-        <<<sms * per_sm, kWavefrontBlock, 0, st>>>(sc, cam, hdr, err, queue, ctr);
+        <<<sms * per_sm, kWavefrontBlock, 0, st>>>(sc, cam, hdr, err, queue, ctr, aux, refill);
     return cudaGetLastError();
+}
+
+template <class R, int MODE, bool COUNT>
+static cudaError_t launch_wave(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
+                               unsigned* queue, unsigned long long* ctr, float4* aux, const Tuning& tn,
+                               cudaStream_t st) {
+    const int refill = tn.refill_min < 1 ? 1 : (tn.refill_min > 32 ? 32 : tn.refill_min);
+    if constexpr (std::is_same<R, float>::value && MODE == 0 && !COUNT) {
+        switch (tn.blocks_per_sm) {
+            case 3: return launch_wave_minb<R, MODE, COUNT, 3>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
+            case 5: return launch_wave_minb<R, MODE, COUNT, 5>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
+            case 6: return launch_wave_minb<R, MODE, COUNT, 6>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
+            default: break;
+        }
+    }
+    return launch_wave_minb<R, MODE, COUNT, WaveDefaults<R>::minb>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
 }
 
 template <class R, int MODE>
 static cudaError_t launch_typed(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
-                                uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx,
-                                int by, cudaStream_t st) {
+                                uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
+                                const Tuning& tn, int bx, int by, cudaStream_t st) {
     if (schedule == 0)
-        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, bx, by, st)
-                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, bx, by, st);
-    return ctr ? launch_wave<R, MODE, true>(sc, cam, hdr, err, queue, ctr, st)
-               : launch_wave<R, MODE, false>(sc, cam, hdr, err, queue, ctr, st);
+        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, aux, bx, by, st)
+                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, aux, bx, by, st);
+    return ctr ? launch_wave<R, MODE, true>(sc, cam, hdr, err, queue, ctr, aux, tn, st)
+               : launch_wave<R, MODE, false>(sc, cam, hdr, err, queue, ctr, aux, tn, st);
 }
 
 cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
-                         uint32_t* err, unsigned* queue, unsigned long long* ctr, int bx, int by,
-                         cudaStream_t st) {
+                         uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
+                         const Tuning& tn, int bx, int by, cudaStream_t st) {
     if (sc.width <= 0 || sc.height <= 0) return cudaSuccess;
-    if (sc.precision == 2) return launch_typed<double, 1>(sc, cam, schedule, hdr, err, queue, ctr, bx, by, st);
-    if (sc.mode == 1) return launch_typed<float, 1>(sc, cam, schedule, hdr, err, queue, ctr, bx, by, st);
-    return launch_typed<float, 0>(sc, cam, schedule, hdr, err, queue, ctr, bx, by, st);
-}
-
-int wavefront_grid(int precision, int device) {
-    int sms = 0, per_sm = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    const void* fn = precision == 2 ? wave_fn<double, 1, false>() : wave_fn<float, 0, false>();
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWavefrontBlock, 0) != cudaSuccess) return 0;
-    return sms * per_sm;
+    if (sc.precision == 2) return launch_typed<double, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
+    if (sc.precision == 1) return launch_typed<Mixed, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
+    if (sc.mode == 1) return launch_typed<float, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
+    return launch_typed<float, 0>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
 }
 
 // =========================================================================================

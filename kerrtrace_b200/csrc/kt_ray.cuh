@@ -56,9 +56,15 @@ struct RayRun {
 };
 
 // Work counters of one ray (only maintained by the counting kernels).
+// Work counters of one ray, and the first shaded disk hit (only maintained by the counting
+// kernels).
 struct Tally {
-    uint32_t steps, attempts, rhs, frozen, fp64;
-    __device__ __forceinline__ void clear() { steps = attempts = rhs = frozen = fp64 = 0; }
+    uint32_t steps, attempts, rhs, frozen, fp64, hits;
+    float first_r, first_g, first_T;
+    __device__ __forceinline__ void clear() {
+        steps = attempts = rhs = frozen = fp64 = hits = 0;
+        first_r = first_g = first_T = __int_as_float(0x7fffffff);
+    }
 };
 
 // Camera ray of sample `sample` of pixel (px, py) (cuda/kernel.cu:108-121): PCG jitter inside
@@ -193,7 +199,7 @@ template <class R, int MODE>
 __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, const R* k1,
                                                const R* k3, const R* k4, const R* k5,
                                                const R* k6, const R* k7, R h, const Scene& sc,
-                                               uint32_t* err) {
+                                               uint32_t* err, Tally* tl) {
     using O = Ops<R>;
     const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
     const R y0 = prev[1], y1 = ry.s[1];
@@ -256,7 +262,13 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
         const R modulator = R(1) + (R)sc.noise_strength * (nval - R(0.5));
         T *= modulator;
     }
+    if (tl && tl->hits == 0) {
+        tl->first_r = (float)rh;
+        tl->first_g = (float)g;
+        tl->first_T = (float)T;
+    }
     if (O::isfiniter(T) && T > R(0)) {
+        if (tl) tl->hits++;
         if constexpr (sizeof(R) == 4) {
             const float3 c = blackbody_rgb<MODE>(T, sc, err);
             const float luma = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
@@ -356,7 +368,7 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     const R r_now = ks_radius<R>(ry.s[0], ry.s[1], ry.s[2], aa);
     if (inside_horizon<R>(r_now, sc)) return true;
     if ((prev[1] < R(0) && ry.s[1] >= R(0)) || (prev[1] > R(0) && ry.s[1] <= R(0)))
-        shade_crossing<R, MODE>(ry, prev, ry.k1, k3, k4, k5, k6, k7, h, sc, err);
+        shade_crossing<R, MODE>(ry, prev, ry.k1, k3, k4, k5, k6, k7, h, sc, err, COUNT ? &tl : nullptr);
     if (ok) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) ry.k1[c] = k7[c];
@@ -377,6 +389,281 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     }
     ry.step++;
     return !(ry.step < sc.max_steps && ry.tau > sc.cutoff_gt);
+}
+
+// =========================================================================================
+// Mixed precision (stated physics only).  The state is a float pair: hi carries every FP32
+// computation (right-hand sides, stages, tests), lo the part of an FP64 value below hi.
+// Outside the photon zone (Kerr-Schild radius of the step start >= sc.zone_r, 1.5 x the
+// retrograde photon-orbit radius) lo is 0 and the step is exactly the FP32 step.  Inside it the
+// state update x + h sum b_i k_i and the embedded error norm run in FP64 on hi + lo, every
+// accepted step renormalises p onto the null cone in FP64, and the result is split back into
+// hi and lo.  The crossing root and the shading run in FP64.
+// =========================================================================================
+struct Mixed {};
+
+template <>
+struct RayRun<Mixed> {
+    float s[6];   // hi
+    float lo[6];  // lo (0 outside the zone)
+    float k1[6];
+    double pt, kt;
+    float h, tol;
+    float col[3];
+    float tau;
+    int step, attempt;
+    bool have_k1, zone;
+};
+
+// Rescales p so that H(x, p) = 0 exactly: with H = (|p|^2 - pt^2 - 2 Hk (l.p - pt)^2) / 2 and
+// p -> lambda p, lambda solves (|p|^2 - 2 Hk (l.p)^2) lambda^2 + 4 Hk pt (l.p) lambda
+// - pt^2 (1 + 2 Hk) = 0; the root next to 1 is taken (no change when none is within 1e-3).
+__device__ __forceinline__ void null_renormalise(double* s, double pt, const Scene& sc) {
+    const double a = sc.a_d, aa = sc.aa_d, M = sc.M_d;
+    const double x = s[0], y = s[1], z = s[2];
+    const double r = ks_radius<double>(x, y, z, aa);
+    const double r2 = r * r, D = r2 + aa;
+    const double lx = (r * x - a * z) / D, ly = y / r, lz = (r * z + a * x) / D;
+    const double Hk = M * r2 * r / (r2 * r2 + aa * y * y);
+    const double lp = lx * s[3] + ly * s[4] + lz * s[5];
+    const double pp = s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+    const double A = pp - 2.0 * Hk * lp * lp;
+    const double B = 4.0 * Hk * pt * lp;
+    const double Cq = -pt * pt * (1.0 + 2.0 * Hk);
+    const double disc = B * B - 4.0 * A * Cq;
+    if (!(A > 0.0) || !(disc >= 0.0)) return;
+    const double sq = sqrt(disc);
+    const double l1 = (-B + sq) / (2.0 * A), l2 = (-B - sq) / (2.0 * A);
+    const double lam = fabs(l1 - 1.0) < fabs(l2 - 1.0) ? l1 : l2;
+    if (!(fabs(lam - 1.0) < 1e-3)) return;
+    s[3] *= lam;
+    s[4] *= lam;
+    s[5] *= lam;
+}
+
+// The start is the FP32 start (the camera and direction are FP32 data; it runs once per ray in
+// the refill path, where FP64 square roots and divisions would cost as much as the ray's steps).
+__device__ __forceinline__ bool ray_start_mixed(RayRun<Mixed>& ry, const Camera& cam, const float dir[3],
+                                                const Scene& sc) {
+    RayRun<float> d;
+    const bool run = ray_start<float>(d, cam, dir, sc);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        ry.s[c] = d.s[c];
+        ry.lo[c] = 0.0f;
+    }
+    ry.pt = (double)d.pt;
+    ry.kt = (double)d.kt;
+    ry.h = d.h;
+    ry.tol = 0.0f;
+    ry.col[0] = ry.col[1] = ry.col[2] = 0.0f;
+    ry.tau = 1.0f;
+    ry.step = 0;
+    ry.attempt = 0;
+    ry.have_k1 = false;
+    ry.zone = false;
+    return run;
+}
+
+// Disk crossing of a mixed-precision step, shaded in FP64 from the hi/lo states.  Kept out of
+// line: it runs on few steps and would otherwise raise the register count of the whole loop.
+// ks rows: k1, k3, k4, k5, k6, k7, lo of the step start.
+static __device__ __noinline__ void shade_mixed(RayRun<Mixed>& ry, const float* prev, const float (*ks)[6], float h,
+                                         const Scene& sc, uint32_t* err, Tally* tl) {
+    RayRun<double> dr;
+    double pd[6], k1d[6], k3d[6], k4d[6], k5d[6], k6d[6], k7d[6];
+    for (int c = 0; c < 6; ++c) {
+        pd[c] = (double)prev[c] + (double)ks[6][c];
+        dr.s[c] = (double)ry.s[c] + (double)ry.lo[c];
+        k1d[c] = ks[0][c];
+        k3d[c] = ks[1][c];
+        k4d[c] = ks[2][c];
+        k5d[c] = ks[3][c];
+        k6d[c] = ks[4][c];
+        k7d[c] = ks[5][c];
+    }
+    dr.pt = ry.pt;
+    dr.kt = ry.kt;
+    dr.col[0] = ry.col[0];
+    dr.col[1] = ry.col[1];
+    dr.col[2] = ry.col[2];
+    dr.tau = ry.tau;
+    shade_crossing<double, 1>(dr, pd, k1d, k3d, k4d, k5d, k6d, k7d, (double)h, sc, err, tl);
+    ry.col[0] = dr.col[0];
+    ry.col[1] = dr.col[1];
+    ry.col[2] = dr.col[2];
+    ry.tau = dr.tau;
+}
+
+template <int MODE, bool COUNT>
+__device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene& sc, uint32_t* err,
+                                                  Tally& tl) {
+    constexpr bool EXACT = true;
+    using O = Ops<float>;
+    using C = DP<float>;
+    using CD = DP<double>;
+    const float a = sc.a, aa = sc.aa, M = sc.M;
+    const float pt = (float)ry.pt;
+    if (ry.attempt == 0) {
+        ry.tol = step_tolerance<float, 1>(ry.s, sc);
+        const bool zone = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa) < sc.zone_r;
+        if (!zone && ry.zone) {  // leaving the zone: fold lo into hi
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                ry.s[c] = (float)((double)ry.s[c] + (double)ry.lo[c]);
+                ry.lo[c] = 0.0f;
+            }
+            ry.have_k1 = false;
+        }
+        ry.zone = zone;
+    }
+    if (!ry.have_k1) {
+        hamilton_rhs<float, EXACT>(ry.s, pt, a, aa, M, ry.k1);
+        ry.have_k1 = true;
+        if (COUNT) tl.rhs++;
+    }
+    const float h = ry.h;
+    const float* s = ry.s;
+    const float* k1 = ry.k1;
+    float y[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], nx[6], inc[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * C::a21 * k1[c];
+    hamilton_rhs<float, EXACT>(y, pt, a, aa, M, k2);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a31 * k1[c] + C::a32 * k2[c]);
+    hamilton_rhs<float, EXACT>(y, pt, a, aa, M, k3);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a41 * k1[c] + C::a42 * k2[c] + C::a43 * k3[c]);
+    hamilton_rhs<float, EXACT>(y, pt, a, aa, M, k4);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        y[c] = s[c] + h * (C::a51 * k1[c] + C::a52 * k2[c] + C::a53 * k3[c] + C::a54 * k4[c]);
+    hamilton_rhs<float, EXACT>(y, pt, a, aa, M, k5);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        y[c] = s[c] + h * (C::a61 * k1[c] + C::a62 * k2[c] + C::a63 * k3[c] + C::a64 * k4[c] + C::a65 * k5[c]);
+    hamilton_rhs<float, EXACT>(y, pt, a, aa, M, k6);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        inc[c] = C::b1 * k1[c] + C::b3 * k3[c] + C::b4 * k4[c] + C::b5 * k5[c] + C::b6 * k6[c];
+        nx[c] = s[c] + h * inc[c];
+    }
+    hamilton_rhs<float, EXACT>(nx, pt, a, aa, M, k7);
+    float errv;
+    if (ry.zone) {
+        double em = 0.0;
+        bool any = false;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double e = (double)h * (CD::e1 * (double)k1[c] + CD::e3 * (double)k3[c] + CD::e4 * (double)k4[c] +
+                                          CD::e5 * (double)k5[c] + CD::e6 * (double)k6[c] + CD::e7 * (double)k7[c]);
+            const double sd = (double)s[c] + (double)ry.lo[c];
+            const double ec = fabs(e) / ((double)ry.tol * fmax(fabs(sd), 1.0));
+            if (ec == ec) {
+                em = any ? fmax(em, ec) : ec;
+                any = true;
+            }
+        }
+        errv = any ? (float)em : __int_as_float(0x7fffffff);
+        if (COUNT) tl.fp64++;
+    } else {
+        float e[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const float scale = ry.tol * O::maxr(O::absr(s[c]), 1.0f);
+            e[c] = O::absr(h * (C::e1 * k1[c] + C::e3 * k3[c] + C::e4 * k4[c] + C::e5 * k5[c] + C::e6 * k6[c] +
+                                C::e7 * k7[c])) / scale;
+        }
+        errv = O::maxr(O::maxr(O::maxr(e[0], e[1]), O::maxr(e[2], e[3])), O::maxr(e[4], e[5]));
+    }
+    const bool ok = errv <= 1.0f;
+    ry.h = h * 0.9f * O::powr(errv, -0.2f);
+    ry.attempt++;
+    if (COUNT) {
+        tl.attempts++;
+        tl.rhs += 6;
+    }
+    if (!ok && ry.attempt < sc.max_attempts) return false;
+
+    float prev[6], prev_lo[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        prev[c] = ry.s[c];
+        prev_lo[c] = ry.lo[c];
+    }
+    if (ry.zone) {
+        double nd[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) nd[c] = ((double)prev[c] + (double)prev_lo[c]) + (double)h * (double)inc[c];
+        if (ok) null_renormalise(nd, ry.pt, sc);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            ry.s[c] = (float)nd[c];
+            ry.lo[c] = (float)(nd[c] - (double)ry.s[c]);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ry.s[c] = nx[c];
+    }
+    ry.attempt = 0;
+    if (COUNT) tl.steps++;
+    if (O::isnanr(ry.s[1])) {
+        if (COUNT) tl.frozen = 1;
+        return true;
+    }
+    const float r_now = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa);
+    if (inside_horizon<float>(r_now, sc)) return true;
+    if ((prev[1] < 0.0f && ry.s[1] >= 0.0f) || (prev[1] > 0.0f && ry.s[1] <= 0.0f)) {
+        float ks[7][6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            ks[0][c] = k1[c];
+            ks[1][c] = k3[c];
+            ks[2][c] = k4[c];
+            ks[3][c] = k5[c];
+            ks[4][c] = k6[c];
+            ks[5][c] = k7[c];
+            ks[6][c] = prev_lo[c];
+        }
+        shade_mixed(ry, prev, ks, h, sc, err, COUNT ? &tl : nullptr);
+    }
+    if (ok) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ry.k1[c] = k7[c];
+        ry.have_k1 = true;
+    } else {
+        ry.have_k1 = false;
+    }
+    if (beyond_escape<float>(r_now, sc)) {
+        float ke[6];
+        hamilton_rhs<float, EXACT>(ry.s, pt, a, aa, M, ke);
+        if (COUNT) tl.rhs++;
+        const float inv = O::rsq(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
+        const float sky = sky_value<float>(ke[0] * inv, ke[1] * inv, ke[2] * inv, ry.tau, sc);
+        ry.col[0] += sky;
+        ry.col[1] += sky;
+        ry.col[2] += sky;
+        return true;
+    }
+    ry.step++;
+    return !(ry.step < sc.max_steps && ry.tau > sc.cutoff_gt);
+}
+
+// Uniform entry points used by the kernels for every arithmetic type.
+template <class R>
+__device__ __forceinline__ bool start(RayRun<R>& ry, const Camera& cam, const float dir[3], const Scene& sc) {
+    return ray_start<R>(ry, cam, dir, sc);
+}
+__device__ __forceinline__ bool start(RayRun<Mixed>& ry, const Camera& cam, const float dir[3], const Scene& sc) {
+    return ray_start_mixed(ry, cam, dir, sc);
+}
+template <int MODE, bool COUNT, class R>
+__device__ __forceinline__ bool advance(RayRun<R>& ry, const Scene& sc, uint32_t* err, Tally& tl) {
+    return ray_advance<R, MODE, COUNT>(ry, sc, err, tl);
+}
+template <int MODE, bool COUNT>
+__device__ __forceinline__ bool advance(RayRun<Mixed>& ry, const Scene& sc, uint32_t* err, Tally& tl) {
+    return ray_advance_mixed<MODE, COUNT>(ry, sc, err, tl);
 }
 
 }  // namespace ktd

@@ -20,7 +20,9 @@ def _peak_scale(cfg: KtConfig, peak_temp: float) -> float:
     """disk_temperature_scale that puts the largest disk-LUT entry at `peak_temp` kelvin (the
     reference scales an un-normalised f^(1/4), src/renderer/utils.rs:172-201)."""
     lut = generate_disk_lut(build_kerr_params(cfg), cfg.disk_outer_radius, cfg.lut_size)
-    return float(peak_temp / float(lut.max()))
+    peak = float(lut.max())
+    # the reference's flux formula is identically 0 for some negative spins: no disk emission
+    return float(peak_temp / peak) if peak > 0 else 0.0
 
 
 def _horizon_eps(cfg: KtConfig, factor: float) -> float:
@@ -117,7 +119,41 @@ def t2() -> tuple[KtConfig, KtCamera]:
     return c, orbit_camera(40.0, 60.0, 70.0, azimuth_deg=30.0)
 
 
-SCENES = {"c1": c1, "c2": c2, "t1": t1, "t2": t2}
+def c3_draws(n: int = 8, seed: int = 7) -> list[tuple[float, float]]:
+    """(spin, inclination in degrees) of the mixed-precision ablation: spin ~ U[-0.99, 0.99],
+    inclination ~ U[5, 89], drawn in that order per draw from numpy's default generator."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [(float(rng.uniform(-0.99, 0.99)), float(rng.uniform(5.0, 89.0))) for _ in range(n)]
+
+
+def c3(draw: int = 0, size: int = 4096) -> tuple[KtConfig, KtCamera]:
+    """Mixed-precision ablation scene: 4096x4096, FOV 20, r_obs 60, 1 spp, stated physics,
+    mixed precision (switch `precision` for the FP32 / FP64 runs), tolerance 1e-6."""
+    spin, incl = c3_draws()[draw]
+    c = config_default()
+    c.width = c.height = size
+    c.spp = 1
+    c.mode, c.precision = 1, 1
+    c.spin, c.mass = spin, 1.0
+    c.tolerance = 1e-6
+    c.initial_step = 0.1
+    c.max_steps = 20000
+    c.max_attempts = 3
+    c.escape_radius = 1000.0
+    c.horizon_epsilon = _horizon_eps(c, 0.01)
+    c.disk_outer_radius = 30.0
+    c.lut_size = 4096
+    c.wavelength_start, c.wavelength_end, c.wavelength_step = 380.0, 720.0, 10.0
+    c.lut_max_temp = 2e5
+    c.disk_temperature_scale = _peak_scale(c, 1e4)
+    c.exposure_scale = 3e-3
+    c.noise_enabled = 0
+    c.bloom_enabled = 0
+    return c, orbit_camera(60.0, incl, 20.0)
+
+
+SCENES = {"c1": c1, "c2": c2, "t1": t1, "t2": t2, "c3": c3}
 
 
 def scene(name: str) -> tuple[KtConfig, KtCamera]:

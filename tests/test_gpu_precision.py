@@ -1,0 +1,84 @@
+"""Stated-physics precision modes on the GPU against the f64 oracle, the per-pixel first-hit
+output of the counting trace, and the launch-shape autotuner."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import kerrtrace_b200 as kt
+from kerrtrace_b200 import autotune, workloads
+from tests.helpers import oracle_parity, run_ours
+
+pytestmark = pytest.mark.gpu
+
+
+def traced(torch, cfg, cam, aux=True, schedule=kt.SCHED_WAVEFRONT):
+    ctx = kt.Context(cfg)
+    n = cfg.width * cfg.height
+    hdr = torch.zeros((n, 4), device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    a = torch.zeros((n, 4), device="cuda")
+    st = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), 0, schedule, a.data_ptr() if aux else 0)
+    torch.cuda.synchronize()
+    return hdr.cpu().numpy(), a.cpu().numpy(), st
+
+
+@pytest.mark.parametrize("prec", [kt.PREC_FP32, kt.PREC_MIXED, kt.PREC_FP64])
+def test_spec_precisions_match_f64_oracle(cuda, orc, prec):
+    cfg, cam = workloads.scene("t1")
+    cfg.mode, cfg.precision = kt.MODE_SPEC, prec
+    hdr, aux, st = traced(cuda, cfg, cam)
+    exp, info, _ = orc.Scene(cfg, cam, tex_mode=0).render(2)
+    r = oracle_parity(hdr, exp, cfg)
+    print(prec, r, "fp64 zone steps", st.fp64_steps, "of", st.steps)
+    assert r["class_mismatch"] <= 0.002 * r["n"], r
+    assert r["over_1e-3"] <= 0.01 * r["n"], r
+    assert r["p99"] <= 1e-3, r
+    if prec == kt.PREC_MIXED:
+        assert 0 < st.fp64_steps < st.steps
+    else:
+        assert st.fp64_steps == 0
+
+
+def test_mixed_schedules_agree(cuda):
+    cfg, cam = workloads.scene("t2")
+    cfg.mode, cfg.precision = kt.MODE_SPEC, kt.PREC_MIXED
+    a, _, _, ctx = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    b, _, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_WAVEFRONT, ctx=ctx)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_first_hit_output_matches_oracle(cuda, orc):
+    """Radius, redshift and temperature of the first shaded disk hit (reference semantics, spp 1
+    scene) against the oracle's per-ray record."""
+    cfg, cam = workloads.scene("c2")
+    cfg = workloads.scaled(cfg, 240, 135)
+    hdr, aux, _ = traced(cuda, cfg, cam)
+    _, info, _ = orc.Scene(cfg, cam, tex_mode=1).render(0)
+    both = np.isfinite(aux[:, 0]) & np.isfinite(info["first_r"])
+    only = np.isfinite(aux[:, 0]) != np.isfinite(info["first_r"])
+    assert both.sum() > 100
+    assert only.sum() <= 0.002 * len(aux)
+    for k, col in (("first_r", 0), ("first_g", 1), ("first_T", 2)):
+        a, b = aux[both, col].astype(np.float64), info[k][both]
+        ok = np.isfinite(a) & np.isfinite(b) & (b != 0)   # T is NaN or 0 where the hit did not shade
+        rel = np.abs(a[ok] - b[ok]) / np.abs(b[ok])
+        assert np.quantile(rel, 0.99) < 1e-3, (k, np.quantile(rel, 0.99))
+    assert np.all(aux[both, 3] >= 0) and np.mean(aux[both, 3] >= 1) > 0.9
+
+
+def test_autotune_picks_an_identical_and_fastest_shape(cuda):
+    cfg, cam = workloads.scene("c2")
+    cfg = workloads.scaled(cfg, 480, 270)
+    ctx = kt.Context(cfg)
+    res = autotune.autotune(ctx, cam, reps=2)
+    assert all(ok for _, _, ok in res.table), [c for _, c, ok in res.table if not ok]
+    assert res.best_ms == min(ms for ms, _, _ in res.table)
+    t = ctx.tuning()
+    assert t.schedule == res.best["schedule"] and t.refill_min == res.best["refill_min"]
+    # KT_SCHED_AUTO now runs the tuned shape and still renders the reference image
+    a, _, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_AUTO, ctx=ctx)
+    b, _, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    with pytest.raises(kt.KtError):
+        ctx.set_tuning(schedule=kt.SCHED_WAVEFRONT, blocks_per_sm=9)
