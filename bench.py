@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--schedule", default="auto", choices=["auto", "wavefront", "plain"])
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--size", default=None, help="WxH override of the scene resolution (same scene otherwise)")
@@ -244,6 +245,40 @@ def precision_leg(cfg, cam, local, reps: int) -> dict:
     return runs
 
 
+def batch_leg(local, reps: int) -> dict:
+    """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
+    random spins, inclinations, observer and disk radii): one batched launch, the same launch
+    replayed from a CUDA graph, and the baseline of 64 sequential plain launches."""
+    import torch
+
+    import kerrtrace_b200 as kt
+    from kerrtrace_b200 import workloads
+
+    jobs = workloads.c4_jobs()
+    bufs = [(torch.zeros((c.width * c.height, 4), device="cuda"), torch.zeros(2, dtype=torch.int32, device="cuda"))
+            for c, _ in jobs]
+    b = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(jobs, bufs)], local)
+    rays = b.rays()
+    stream = torch.cuda.current_stream().cuda_stream
+    out = {"jobs": len(jobs), "rays": rays}
+    for name, fn in (("sequential_plain", lambda: b.trace_sequential(stream, kt.SCHED_PLAIN)),
+                     ("batched_launch", lambda: b.trace(stream)),
+                     ("batched_graph", lambda: b.trace_graph(stream))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": round(ms, 3), "mrays_s": round(rays / ms / 1e3, 1)}
+    out["speedup_graph_vs_sequential"] = round(out["sequential_plain"]["ms"] / out["batched_graph"]["ms"], 3)
+    b.close()
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -358,6 +393,8 @@ def run_ours(args, rank, world, local):
         line["autotune"] = tuned.summary()
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision"] = precision_leg(cfg, cam, local, max(3, args.steps))
+    if rank == 0 and world == 1 and not args.no_batch:
+        line["batch"] = batch_leg(local, 3)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, cam, args.cpu_seconds)
     if rank == 0:

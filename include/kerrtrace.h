@@ -234,6 +234,33 @@ kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const
  * kt_bloom_horizontal followed by kt_post_process. */
 kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_t* image_out);
 
+/* ---- batched renders (many scenes / cameras in one launch) -------------------------------- */
+/* Largest number of renders in one batch (the job table is a kernel parameter). */
+#define KT_BATCH_MAX_JOBS 64
+/* One render of a batch: its own scene (spin, disk, resolution, ...), camera and outputs.
+ * All jobs of a batch share `mode` and `precision`. */
+typedef struct kt_job {
+    kt_config cfg;
+    kt_camera cam;
+    float* hdr_out;      /* dev float[4*W*H] */
+    uint32_t* err_word;  /* dev uint32[2], not cleared by the trace calls */
+} kt_job;
+typedef struct kt_batch kt_batch;
+/* Builds one context per job (its LUTs and textures) and the launch table. */
+kt_status kt_batch_create(const kt_job* jobs, uint32_t n_jobs, int device, kt_batch** out);
+/* Plain-schedule block shape of the batched launch (default 16x16; at most 1024 threads). */
+kt_status kt_batch_set_block(kt_batch* b, int32_t block_x, int32_t block_y);
+/* New camera for job j (the next kt_batch_trace_graph re-captures its graph). */
+kt_status kt_batch_set_camera(kt_batch* b, uint32_t j, const kt_camera* cam);
+/* Traces every job in one kernel launch on `stream`. */
+kt_status kt_batch_trace(kt_batch* b, void* stream);
+/* The same launch replayed from a CUDA graph, captured on first use (and after a change). */
+kt_status kt_batch_trace_graph(kt_batch* b, void* stream);
+/* Baseline: one kt_trace launch per job, in job order, on `stream`. */
+kt_status kt_batch_trace_sequential(kt_batch* b, void* stream, int32_t schedule);
+uint64_t kt_batch_rays(const kt_batch* b);
+void kt_batch_destroy(kt_batch* b);
+
 /* ---- trace without any device allocation --------------------------------------------------- */
 /* Largest n_views of one kt_trace_noalloc call: its scratch is one 32-bit work counter per view,
  * held in a 256-byte array inside the library's device image. */

@@ -30,6 +30,7 @@ MODE_REF, MODE_SPEC = 0, 1
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
 SCHED_PLAIN, SCHED_WAVEFRONT, SCHED_AUTO = 0, 1, 2
 NOALLOC_MAX_VIEWS = 64
+BATCH_MAX_JOBS = 64
 
 
 class KtConfig(C.Structure):
@@ -96,6 +97,12 @@ class KtTuning(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class KtJob(C.Structure):
+    """Mirror of ``kt_job``: one render of a batch."""
+
+    _fields_ = [("cfg", KtConfig), ("cam", KtCamera), ("hdr_out", C.c_void_p), ("err_word", C.c_void_p)]
+
+
 class KtError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"kerrtrace status {status}: {message}")
@@ -136,6 +143,14 @@ SIGNATURES = [
     ("kt_post_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_trace_noalloc", C.c_int, [C.POINTER(KtConfig), C.POINTER(KtCamera), C.c_uint32, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_batch_create", C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
+    ("kt_batch_set_block", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    ("kt_batch_set_camera", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(KtCamera)]),
+    ("kt_batch_trace", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("kt_batch_trace_graph", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("kt_batch_trace_sequential", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    ("kt_batch_rays", C.c_uint64, [C.c_void_p]),
+    ("kt_batch_destroy", None, [C.c_void_p]),
     ("kt_renderer_new", C.c_int, [C.POINTER(KtConfig), C.c_int, C.POINTER(C.c_void_p)]),
     ("kt_renderer_submit_render", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                             C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
@@ -299,6 +314,51 @@ class Context:
     def close(self):
         if self.handle:
             lib().kt_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many renders (scenes, cameras, resolutions) traced in one launch (kt_batch_*)."""
+
+    def __init__(self, jobs: list, device: int = 0):
+        """jobs: list of (KtConfig, KtCamera, hdr_dev_ptr, err_dev_ptr)."""
+        arr = (KtJob * len(jobs))()
+        for i, (cfg, cam, hdr, err) in enumerate(jobs):
+            arr[i].cfg = cfg
+            arr[i].cam = cam
+            arr[i].hdr_out = hdr
+            arr[i].err_word = err
+        h = C.c_void_p()
+        check(lib().kt_batch_create(arr, len(jobs), device, C.byref(h)))
+        self.handle = h
+
+    def rays(self) -> int:
+        return int(lib().kt_batch_rays(self.handle))
+
+    def set_block(self, bx: int, by: int):
+        check(lib().kt_batch_set_block(self.handle, bx, by))
+
+    def set_camera(self, j: int, cam: KtCamera):
+        check(lib().kt_batch_set_camera(self.handle, j, C.byref(cam)))
+
+    def trace(self, stream: int = 0):
+        check(lib().kt_batch_trace(self.handle, C.c_void_p(stream)))
+
+    def trace_graph(self, stream: int = 0):
+        check(lib().kt_batch_trace_graph(self.handle, C.c_void_p(stream)))
+
+    def trace_sequential(self, stream: int = 0, schedule: int = SCHED_PLAIN):
+        check(lib().kt_batch_trace_sequential(self.handle, C.c_void_p(stream), schedule))
+
+    def close(self):
+        if self.handle:
+            lib().kt_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

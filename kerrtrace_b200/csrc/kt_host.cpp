@@ -985,3 +985,162 @@ kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hd
 void kt_renderer_destroy(kt_renderer* r) { destroy_renderer(r); }
 
 }  // extern "C"
+
+// =========================================================================================
+// Batched renders
+// =========================================================================================
+struct kt_batch {
+    int device = 0;
+    std::vector<kt_context*> ctx;
+    std::vector<kt_job> jobs;
+    ktd::BatchTable* table = nullptr;
+    int bx = 16, by = 16;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t capture = nullptr;
+};
+
+namespace {
+void batch_drop_graph(kt_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+void batch_layout(kt_batch* b) {
+    int tiles = 0;
+    for (int j = 0; j < b->table->n; ++j) {
+        ktd::BatchJob& e = b->table->job[j];
+        e.tiles_x = (e.sc.width + b->bx - 1) / b->bx;
+        const int tiles_y = (e.sc.height + b->by - 1) / b->by;
+        e.tile_begin = tiles;
+        tiles += e.tiles_x * tiles_y;
+    }
+    b->table->total_tiles = tiles;
+}
+void batch_free(kt_batch* b) {
+    if (!b) return;
+    {
+        DeviceGuard g(b->device);
+        batch_drop_graph(b);
+        if (b->capture) cudaStreamDestroy(b->capture);
+    }
+    for (kt_context* c : b->ctx) destroy_ctx(c);
+    delete b->table;
+    delete b;
+}
+}  // namespace
+
+extern "C" {
+
+kt_status kt_batch_create(const kt_job* jobs, uint32_t n, int device, kt_batch** out) {
+    if (!jobs || !out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    *out = nullptr;
+    if (n == 0 || n > KT_BATCH_MAX_JOBS)
+        return fail(KT_ERR_INVALID_ARG, "a batch holds 1..%d jobs, got %u", KT_BATCH_MAX_JOBS, n);
+    for (uint32_t j = 0; j < n; ++j) {
+        if (!jobs[j].hdr_out || !jobs[j].err_word) return fail(KT_ERR_INVALID_ARG, "job %u: NULL output", j);
+        if (jobs[j].cfg.mode != jobs[0].cfg.mode || jobs[j].cfg.precision != jobs[0].cfg.precision)
+            return fail(KT_ERR_INVALID_ARG, "job %u: every job of a batch must share mode and precision", j);
+    }
+    kt_batch* b = new (std::nothrow) kt_batch();
+    if (!b) return fail(KT_ERR_INVALID_ARG, "out of host memory");
+    b->device = device;
+    b->table = new (std::nothrow) ktd::BatchTable();
+    if (!b->table) {
+        delete b;
+        return fail(KT_ERR_INVALID_ARG, "out of host memory");
+    }
+    b->jobs.assign(jobs, jobs + n);
+    b->table->n = (int)n;
+    for (uint32_t j = 0; j < n; ++j) {
+        kt_context* c = nullptr;
+        const kt_status st = kt_context_create(&jobs[j].cfg, device, &c);
+        if (st != KT_OK) {
+            batch_free(b);
+            return st;
+        }
+        b->ctx.push_back(c);
+        ktd::BatchJob& e = b->table->job[j];
+        e.sc = c->scene;
+        e.cam = to_camera(&jobs[j].cam);
+        e.hdr = reinterpret_cast<float4*>(jobs[j].hdr_out);
+        e.err = jobs[j].err_word;
+    }
+    batch_layout(b);
+    *out = b;
+    return KT_OK;
+}
+
+kt_status kt_batch_set_block(kt_batch* b, int32_t bx, int32_t by) {
+    if (!b) return fail(KT_ERR_INVALID_ARG, "batch is NULL");
+    if (bx <= 0 || by <= 0 || (int64_t)bx * by > 1024) return fail(KT_ERR_INVALID_ARG, "block %dx%d invalid", bx, by);
+    b->bx = bx;
+    b->by = by;
+    batch_layout(b);
+    batch_drop_graph(b);
+    return KT_OK;
+}
+
+kt_status kt_batch_set_camera(kt_batch* b, uint32_t j, const kt_camera* cam) {
+    if (!b || !cam) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if ((int)j >= b->table->n) return fail(KT_ERR_INVALID_ARG, "job %u out of range", j);
+    b->jobs[j].cam = *cam;
+    b->table->job[j].cam = to_camera(cam);
+    batch_drop_graph(b);
+    return KT_OK;
+}
+
+kt_status kt_batch_trace(kt_batch* b, void* stream) {
+    if (!b) return fail(KT_ERR_INVALID_ARG, "batch is NULL");
+    DeviceGuard g(b->device);
+    const cudaError_t e = ktd::launch_batch(*b->table, b->bx, b->by, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+    return KT_OK;
+}
+
+kt_status kt_batch_trace_graph(kt_batch* b, void* stream) {
+    if (!b) return fail(KT_ERR_INVALID_ARG, "batch is NULL");
+    DeviceGuard g(b->device);
+    if (!b->exec) {
+        if (!b->capture) KT_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking), "create capture stream");
+        KT_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal), "begin capture");
+        const cudaError_t le = ktd::launch_batch(*b->table, b->bx, b->by, b->capture);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->capture, &graph);
+        if (le != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return cuda_fail(le, "batch launch under capture");
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "end capture");
+        b->graph = graph;
+        const cudaError_t ie = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        if (ie != cudaSuccess) {
+            batch_drop_graph(b);
+            return cuda_fail(ie, "instantiate graph");
+        }
+    }
+    KT_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream), "launch graph");
+    return KT_OK;
+}
+
+kt_status kt_batch_trace_sequential(kt_batch* b, void* stream, int32_t schedule) {
+    if (!b) return fail(KT_ERR_INVALID_ARG, "batch is NULL");
+    for (size_t j = 0; j < b->ctx.size(); ++j) {
+        const kt_status st = kt_trace(b->ctx[j], stream, &b->jobs[j].cam, schedule, b->jobs[j].hdr_out, b->jobs[j].err_word);
+        if (st != KT_OK) return st;
+    }
+    return KT_OK;
+}
+
+uint64_t kt_batch_rays(const kt_batch* b) {
+    if (!b) return 0;
+    uint64_t r = 0;
+    for (const kt_job& j : b->jobs) r += (uint64_t)j.cfg.width * j.cfg.height * j.cfg.spp;
+    return r;
+}
+
+void kt_batch_destroy(kt_batch* b) { batch_free(b); }
+
+}  // extern "C"
+

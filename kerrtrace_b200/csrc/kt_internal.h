@@ -37,6 +37,25 @@ cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float
                          uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
                          const Tuning& tn, int bx, int by, cudaStream_t stream);
 
+// Batched trace: one plain-schedule launch over the tiles of up to kBatchMaxJobs renders.  The
+// table travels as a kernel parameter (__grid_constant__); each block finds its job from the
+// tile prefix, so the job index and its scene constants are uniform across the block.
+constexpr int kBatchMaxJobs = 64;
+struct BatchJob {
+    Scene sc;
+    Camera cam;
+    float4* hdr;
+    uint32_t* err;
+    int tiles_x;
+    int tile_begin;
+};
+struct BatchTable {
+    BatchJob job[kBatchMaxJobs];
+    int n;
+    int total_tiles;
+};
+cudaError_t launch_batch(const BatchTable& bt, int bx, int by, cudaStream_t stream);
+
 cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, float4* bloom,
                                     cudaStream_t stream);
 cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const float4* bloom,

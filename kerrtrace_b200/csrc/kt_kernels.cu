@@ -74,8 +74,14 @@ __device__ __forceinline__ void run_ray(int px, int py, int smp, const Scene& sc
     }
 }
 
+// Resident 256-thread blocks per SM asked of the compiler for the plain kernel: two for the
+// FP32 and mixed paths (at most 128 registers per thread, 16 warps per SM), one for FP64.
+template <class R> struct PlainMinBlocks { static constexpr int v = 2; };
+template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
+
 template <class R, int MODE, bool COUNT, int MAXT>
-__global__ void __launch_bounds__(MAXT) trace_plain_kernel(const Scene sc, const Camera cam,
+__global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
+    trace_plain_kernel(const Scene sc, const Camera cam,
                                                            float4* __restrict__ hdr,
                                                            uint32_t* __restrict__ err,
                                                            unsigned long long* __restrict__ ctr,
@@ -272,6 +278,46 @@ cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float
     if (sc.precision == 1) return launch_typed<Mixed, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
     if (sc.mode == 1) return launch_typed<float, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
     return launch_typed<float, 0>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
+}
+
+// ---- batched renders -----------------------------------------------------------------------
+template <class R, int MODE, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
+    trace_batch_kernel(const __grid_constant__ BatchTable bt) {
+    const int b = blockIdx.x;
+    int j = 0;
+    while (j + 1 < bt.n && b >= bt.job[j + 1].tile_begin) ++j;
+    const BatchJob& jb = bt.job[j];
+    const Scene& sc = jb.sc;
+    const int t = b - jb.tile_begin;
+    const int ty = t / jb.tiles_x, tx = t - ty * jb.tiles_x;
+    const int px = tx * (int)blockDim.x + (int)threadIdx.x;
+    const int py = ty * (int)blockDim.y + (int)threadIdx.y;
+    if (px >= sc.width || py >= sc.height) return;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    Tally total;
+    total.clear();
+    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, false>(px, py, smp, sc, jb.cam, jb.err, acc, total, nullptr);
+    const float fs = sc.final_scale;
+    jb.hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+}
+
+template <class R, int MODE>
+static cudaError_t launch_batch_typed(const BatchTable& bt, int bx, int by, cudaStream_t st) {
+    if (bx * by <= 256)
+        trace_batch_kernel<R, MODE, 256><<<bt.total_tiles, dim3(bx, by), 0, st>>>(bt);
+    else
+        trace_batch_kernel<R, MODE, 1024><<<bt.total_tiles, dim3(bx, by), 0, st>>>(bt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const BatchTable& bt, int bx, int by, cudaStream_t st) {
+    if (bt.n <= 0 || bt.total_tiles <= 0) return cudaSuccess;
+    const Scene& s0 = bt.job[0].sc;
+    if (s0.precision == 2) return launch_batch_typed<double, 1>(bt, bx, by, st);
+    if (s0.precision == 1) return launch_batch_typed<Mixed, 1>(bt, bx, by, st);
+    if (s0.mode == 1) return launch_batch_typed<float, 1>(bt, bx, by, st);
+    return launch_batch_typed<float, 0>(bt, bx, by, st);
 }
 
 // =========================================================================================

@@ -153,6 +153,31 @@ def c3(draw: int = 0, size: int = 4096) -> tuple[KtConfig, KtCamera]:
     return c, orbit_camera(60.0, incl, 20.0)
 
 
+def c4_jobs(seed: int = 123, scale: int = 1) -> list[tuple[KtConfig, KtCamera]]:
+    """Batched-launch workload: 64 independent renders, 16 each of 256^2, 512^2, 1024^2 and
+    1920x1080 (divided by `scale`), with spin ~ U[-0.99, 0.99], inclination ~ U[5, 89] deg,
+    observer radius ~ U[30, 200] M and disk outer radius ~ U[10, 50] M drawn per job (in that
+    order) from numpy's default generator; tolerance 1e-6, reference semantics."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sizes = [(256, 256)] * 16 + [(512, 512)] * 16 + [(1024, 1024)] * 16 + [(1920, 1080)] * 16
+    jobs = []
+    for w, h in sizes:
+        spin = float(rng.uniform(-0.99, 0.99))
+        incl = float(rng.uniform(5.0, 89.0))
+        r_obs = float(rng.uniform(30.0, 200.0))
+        r_out = float(rng.uniform(10.0, 50.0))
+        c, _ = c2()
+        c.width, c.height = max(8, w // scale), max(8, h // scale)
+        c.spin = spin
+        c.horizon_epsilon = _horizon_eps(c, 0.01)
+        c.disk_outer_radius = r_out
+        c.lut_max_temp = 2e5
+        c.disk_temperature_scale = _peak_scale(c, 1e4)
+        jobs.append((c, orbit_camera(r_obs, incl, 25.0)))
+    return jobs
+
+
 SCENES = {"c1": c1, "c2": c2, "t1": t1, "t2": t2, "c3": c3}
 
 
