@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--schedule", default="auto", choices=["auto", "wavefront", "plain"])
+    ap.add_argument("--mode", default="ref", choices=["ref", "spec"],
+                    help="semantics of the main loop: the reference's (default) or stated physics")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"],
+                    help="arithmetic of the main loop (mixed / fp64 need --mode spec)")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -286,6 +290,8 @@ def run_ours(args, rank, world, local):
     from kerrtrace_b200 import autotune, flops, workloads
 
     cfg, cam = rank_camera(kt, workloads, args.workload, rank, world, args.size)
+    cfg.mode = kt.MODE_SPEC if args.mode == "spec" else kt.MODE_REF
+    cfg.precision = {"fp32": kt.PREC_FP32, "mixed": kt.PREC_MIXED, "fp64": kt.PREC_FP64}[args.precision]
     sched = {"auto": kt.SCHED_AUTO, "wavefront": kt.SCHED_WAVEFRONT, "plain": kt.SCHED_PLAIN}[args.schedule]
     ctx = kt.Context(cfg, local)
     n = cfg.width * cfg.height
@@ -384,8 +390,9 @@ def run_ours(args, rank, world, local):
         "config": {"workload": f"{args.workload}: {cfg.width}x{cfg.height}, a={cfg.spin:.3f}, tol={cfg.tolerance:g}, "
                                f"max_steps={cfg.max_steps}, spp={cfg.spp}, bloom r={cfg.bloom_radius:g}",
                    "schedule": args.schedule, "tuning": t.as_dict(),
-                   "mode": "reference semantics (drop-in, bit-identical to the reference kernel)",
-                   "precision": "fp32", "l2": "flushed between steps (256 MiB write outside the timed events)",
+                   "mode": "reference semantics (drop-in, bit-identical to the reference kernel)" if args.mode == "ref"
+                   else "stated physics", "precision": args.precision,
+                   "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"replica frames x{world}"},
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": 2 * args.steps,
     }
