@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define KT_ABI_VERSION 1
+#define KT_ABI_VERSION 2
 
 typedef enum kt_status {
     KT_OK = 0,
@@ -64,6 +64,14 @@ typedef enum kt_schedule {
     KT_SCHED_AUTO = 2       /* whichever the context's kt_tuning selects (the autotuner's choice) */
 } kt_schedule;
 
+/* Order in which the tracers take pixels.  Per-pixel results are the same in both. */
+typedef enum kt_order {
+    KT_ORDER_TILES = 0,      /* 16x16 tiles in raster order (plain: the 2D grid) */
+    KT_ORDER_LONG_FIRST = 1  /* a rank kernel first moves the pixels whose rays are predicted to
+                                wind near a photon orbit (Kerr constants of motion) to the front,
+                                so the longest rays start first instead of forming the tail */
+} kt_order;
+
 /* Launch shape used by KT_SCHED_AUTO (see kt_context_set_tuning). */
 typedef struct kt_tuning {
     int32_t schedule;      /* KT_SCHED_PLAIN or KT_SCHED_WAVEFRONT */
@@ -71,6 +79,7 @@ typedef struct kt_tuning {
     int32_t block_y;
     int32_t blocks_per_sm; /* wavefront: resident blocks of 128 threads per SM, 3..6 */
     int32_t refill_min;    /* wavefront: idle lanes a warp collects before refilling them, 1..32 */
+    int32_t order;         /* kt_order; KT_ORDER_LONG_FIRST allocates a 4-byte-per-pixel buffer */
 } kt_tuning;
 
 /*
@@ -221,7 +230,9 @@ kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam,
  * per thread accordingly; only the FP32 reference-semantics kernel has the 3/5/6 variants) and
  * the refill threshold.  For the plain schedule: the block shape (at most 1024 threads).
  * kt_trace(KT_SCHED_AUTO) runs tuning->schedule; the explicit schedules use the rest of the
- * tuning too.  Default: wavefront, config block_dim, 4 blocks per SM, refill 1. */
+ * tuning too, the pixel order included.  Default: wavefront, config block_dim, 4 blocks per
+ * SM, refill 1, tile order.  Call it outside stream capture: the first long-first tuning of a
+ * context allocates the order buffer. */
 kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* tuning);
 kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* tuning);
 /* bloom_horizontal (cuda/kernel.cu:144-173): dev float4 hdr -> dev float4 bloom. */

@@ -29,6 +29,7 @@ KT_ERR_TIMEOUT = 8
 MODE_REF, MODE_SPEC = 0, 1
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
 SCHED_PLAIN, SCHED_WAVEFRONT, SCHED_AUTO = 0, 1, 2
+ORDER_TILES, ORDER_LONG_FIRST = 0, 1
 NOALLOC_MAX_VIEWS = 64
 BATCH_MAX_JOBS = 64
 
@@ -91,7 +92,7 @@ class KtTuning(C.Structure):
     """Mirror of ``kt_tuning``: the launch shape that KT_SCHED_AUTO runs."""
 
     _fields_ = [("schedule", C.c_int32), ("block_x", C.c_int32), ("block_y", C.c_int32),
-                ("blocks_per_sm", C.c_int32), ("refill_min", C.c_int32)]
+                ("blocks_per_sm", C.c_int32), ("refill_min", C.c_int32), ("order", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -292,8 +293,8 @@ class Context:
         return st
 
     def set_tuning(self, schedule: int = SCHED_WAVEFRONT, block_x: int = 0, block_y: int = 0,
-                   blocks_per_sm: int = 4, refill_min: int = 1):
-        t = KtTuning(schedule, block_x, block_y, blocks_per_sm, refill_min)
+                   blocks_per_sm: int = 4, refill_min: int = 1, order: int = 0):
+        t = KtTuning(schedule, block_x, block_y, blocks_per_sm, refill_min, order)
         check(lib().kt_context_set_tuning(self.handle, C.byref(t)))
 
     def tuning(self) -> KtTuning:

@@ -8,6 +8,9 @@ candidates are:
   wavefront  persistent blocks; lanes are refilled from a device work counter once `refill_min`
              lanes of a warp are idle (resident blocks per SM = register cap, refill threshold)
 
+each in tile order and in long-rays-first order (a rank kernel moves the pixels whose rays are
+predicted to wind near a photon orbit to the front, so they do not form the frame's tail).
+
 Every candidate must reproduce the first candidate's image bit for bit (they all run the same
 per-ray arithmetic).  The fastest one is installed in the context, and KT_SCHED_AUTO then runs it.
 Timing uses CUDA events on the launch stream, median of `reps` launches after a warm-up launch.
@@ -18,7 +21,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import SCHED_AUTO, SCHED_PLAIN, SCHED_WAVEFRONT, Context, KtCamera
+from . import ORDER_LONG_FIRST, ORDER_TILES, SCHED_AUTO, SCHED_PLAIN, SCHED_WAVEFRONT, Context, KtCamera
 
 PLAIN_BLOCKS = [(16, 16), (32, 8), (8, 8), (16, 8), (32, 4), (8, 16)]
 WAVE_BLOCKS_PER_SM = [3, 4, 5, 6]
@@ -26,12 +29,14 @@ WAVE_REFILL = [1, 4, 8, 16]
 
 
 def candidates(precision: int = 0, mode: int = 0) -> list[dict]:
-    out = [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=4, refill_min=1)
-           for bx, by in PLAIN_BLOCKS]
-    # only the FP32 reference-semantics kernel has the 3/5/6 blocks-per-SM variants
-    bps = WAVE_BLOCKS_PER_SM if (precision == 0 and mode == 0) else [4]
-    out += [dict(schedule=SCHED_WAVEFRONT, block_x=0, block_y=0, blocks_per_sm=b, refill_min=r)
-            for b in bps for r in WAVE_REFILL]
+    out = []
+    for order in (ORDER_TILES, ORDER_LONG_FIRST):
+        out += [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=4, refill_min=1, order=order)
+                for bx, by in PLAIN_BLOCKS]
+        # only the FP32 reference-semantics kernel has the 3/5/6 blocks-per-SM variants
+        bps = WAVE_BLOCKS_PER_SM if (precision == 0 and mode == 0) else [4]
+        out += [dict(schedule=SCHED_WAVEFRONT, block_x=0, block_y=0, blocks_per_sm=b, refill_min=r, order=order)
+                for b in bps for r in WAVE_REFILL]
     return out
 
 

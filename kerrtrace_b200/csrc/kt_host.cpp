@@ -434,6 +434,7 @@ struct kt_context {
     unsigned* queue = nullptr;              // wavefront work counter (1 word)
     ktd::Tuning tuning;                     // persistent-tracer launch shape
     unsigned long long* counters = nullptr; // 6 x u64 for the counting launches
+    unsigned* order = nullptr;              // pixel order (allocated when a tuning asks for it)
     int block_x = 16, block_y = 16;
 };
 
@@ -452,6 +453,7 @@ void destroy_ctx(kt_context* c) {
     cudaFree(c->disk_lut_dev);
     cudaFree(c->queue);
     cudaFree(c->counters);
+    cudaFree(c->order);
     cudaSetDevice(prev);
     delete c;
 }
@@ -550,6 +552,7 @@ kt_status fill_scene(kt_context* c) {
     const double an = std::fmin(std::fabs((double)p.a_norm), 1.0);
     const double rph = 2.0 * s.M_d * (1.0 + std::cos(2.0 / 3.0 * std::acos(an)));
     s.zone_r = (float)(zf * rph);
+    s.zone_err64 = cfg.tolerance < 3e-7f ? 1 : 0;
     s.spec_tol_floor = 1.0f;
     s.width = (int)cfg.width;
     s.height = (int)cfg.height;
@@ -674,6 +677,7 @@ struct DeviceGuard {
 
 int plain_bx(const kt_context* c) { return c->tuning.block_x > 0 ? c->tuning.block_x : c->block_x; }
 int plain_by(const kt_context* c) { return c->tuning.block_y > 0 ? c->tuning.block_y : c->block_y; }
+unsigned* order_buffer(const kt_context* c) { return c->tuning.order == KT_ORDER_LONG_FIRST ? c->order : nullptr; }
 
 ktd::Camera to_camera(const kt_camera* cam) {
     ktd::Camera c;
@@ -715,6 +719,14 @@ kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* t) {
     if (t->block_x < 0 || t->block_y < 0 || (int64_t)t->block_x * t->block_y > 1024 ||
         ((t->block_x == 0) != (t->block_y == 0)))
         return fail(KT_ERR_INVALID_ARG, "plain block %dx%d invalid", t->block_x, t->block_y);
+    if (t->order != KT_ORDER_TILES && t->order != KT_ORDER_LONG_FIRST)
+        return fail(KT_ERR_INVALID_ARG, "tuning order %d must be tiles or long-first", t->order);
+    if (t->order == KT_ORDER_LONG_FIRST && !ctx->order) {
+        DeviceGuard g(ctx->device);
+        const size_t words = ktd::kOrderHeader + (size_t)ctx->cfg.width * ctx->cfg.height;
+        KT_CUDA(cudaMalloc(&ctx->order, words * sizeof(unsigned)), "allocate pixel order");
+    }
+    ctx->tuning.order = t->order;
     ctx->tuning.schedule = t->schedule;
     ctx->tuning.block_x = t->block_x;
     ctx->tuning.block_y = t->block_y;
@@ -729,6 +741,7 @@ kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* t) {
     t->block_y = ctx->tuning.block_y;
     t->blocks_per_sm = ctx->tuning.blocks_per_sm;
     t->refill_min = ctx->tuning.refill_min;
+    t->order = ctx->tuning.order;
     return KT_OK;
 }
 
@@ -740,7 +753,7 @@ kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t 
     const int sched = schedule == KT_SCHED_AUTO ? ctx->tuning.schedule : schedule;
     const cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), sched, reinterpret_cast<float4*>(hdr_out),
                                             err_word, ctx->queue, nullptr, nullptr, ctx->tuning, plain_bx(ctx),
-                                            plain_by(ctx), (cudaStream_t)stream);
+                                            plain_by(ctx), order_buffer(ctx), (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "trace launch");
     return KT_OK;
 }
@@ -758,7 +771,7 @@ kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam, 
                 "clear aux");
     cudaError_t e = ktd::launch_trace(ctx->scene, to_camera(cam), sched, reinterpret_cast<float4*>(hdr_out),
                                       err_word, ctx->queue, ctx->counters, reinterpret_cast<float4*>(aux_out),
-                                      ctx->tuning, plain_bx(ctx), plain_by(ctx), st);
+                                      ctx->tuning, plain_bx(ctx), plain_by(ctx), order_buffer(ctx), st);
     if (e != cudaSuccess) return cuda_fail(e, "trace launch");
     unsigned long long h[8];
     KT_CUDA(cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, st), "read counters");

@@ -27,15 +27,22 @@ struct Tuning {
     int block_x = 0, block_y = 0;
     int blocks_per_sm = 4;
     int refill_min = 1;
+    int order = 0;  // 1: pixels ranked long-rays-first by the rank kernel before the trace
 };
+
+// Pixel-order buffer: kOrderHeader header words (marked / unmarked counts), then one pixel
+// index per work unit.
+constexpr unsigned kOrderHeader = 16;
 
 // Trace launch: schedule 0 = plain 2D grid (block bx x by), 1 = persistent wavefront.
 // precision 0 = FP32, 1 = mixed, 2 = FP64.  queue: one device word, reset here on `stream`.
 // ctr: optional 6 x u64 device counters (selects the counting kernels); aux: optional float4
 // per pixel with the first shaded disk hit (r, g, T, hits) of sample 0 (counting kernels only).
+// order: NULL for tile order, else a pixel-order buffer of kOrderHeader + width * height words
+// that the rank kernel fills on `stream` before the trace.
 cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
                          uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
-                         const Tuning& tn, int bx, int by, cudaStream_t stream);
+                         const Tuning& tn, int bx, int by, unsigned* order, cudaStream_t stream);
 
 // Batched trace: one plain-schedule launch over the tiles of up to kBatchMaxJobs renders.  The
 // table travels as a kernel parameter (__grid_constant__); each block finds its job from the

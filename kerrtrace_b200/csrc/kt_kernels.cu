@@ -74,30 +74,6 @@ __device__ __forceinline__ void run_ray(int px, int py, int smp, const Scene& sc
     }
 }
 
-// Resident 256-thread blocks per SM asked of the compiler for the plain kernel: two for the
-// FP32 and mixed paths (at most 128 registers per thread, 16 warps per SM), one for FP64.
-template <class R> struct PlainMinBlocks { static constexpr int v = 2; };
-template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
-
-template <class R, int MODE, bool COUNT, int MAXT>
-__global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
-    trace_plain_kernel(const Scene sc, const Camera cam,
-                                                           float4* __restrict__ hdr,
-                                                           uint32_t* __restrict__ err,
-                                                           unsigned long long* __restrict__ ctr,
-                                                           float4* __restrict__ aux) {
-    const int px = blockIdx.x * blockDim.x + threadIdx.x;
-    const int py = blockIdx.y * blockDim.y + threadIdx.y;
-    if (px >= sc.width || py >= sc.height) return;
-    float acc[3] = {0.0f, 0.0f, 0.0f};
-    Tally total;
-    total.clear();
-    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total, aux);
-    const float fs = sc.final_scale;
-    hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
-    if (COUNT) add_tally(ctr, (uint64_t)sc.spp, total);
-}
-
 // Work unit -> pixel.  Units run over 16-row bands, 16-column tiles inside a band, row-major
 // inside a tile, so 32 consecutive units form a 16x2 patch (the footprint of one warp of the
 // reference's 16x16 blocks).  Exact bijection onto [0, W) x [0, H), partial tiles included.
@@ -116,6 +92,132 @@ __device__ __forceinline__ void unit_to_pixel(unsigned u, int W, int H, int& px,
     px = col0 + (int)(rem2 % (unsigned)wt);
 }
 
+// ---- long-rays-first pixel order -----------------------------------------------------------
+// A ray that passes close to a spherical photon orbit winds around the hole about ln(1/delta)
+// times before it falls in or escapes, and takes several times the average step count.  Traced
+// last, such rays leave single latency-bound warps running after the rest of the frame is done.
+// The Kerr constants of motion of the initial state (E = -p_t, the angular momentum about the
+// spin axis L = z p_x - x p_z, the Carter constant Q, with p_theta from the spheroidal
+// coordinates of the Kerr-Schild point) fix the radial potential
+//   R(r) = (E (r^2 + a^2) - a L)^2 - (r^2 - 2 M r + a^2) ((L - a E)^2 + Q),
+// whose local minimum outside the horizon is close to 0 exactly for those rays.  The rank kernel
+// marks pixels with |R(r_min)| < kHotThreshold E^2 r_min^4 (0.2% to 4% of a frame) and writes
+// a permutation of the pixels: the marked ones first, then the rest in tile order.  The tracers
+// read it when the tuning's order is 1.  Per-pixel results do not depend on the order.
+constexpr float kHotThreshold = 0.1f;
+
+__device__ __forceinline__ bool predicted_long(const Scene& sc, const Camera& cam, const float dir[3]) {
+    RayRun<float> ry;
+    ray_start<float>(ry, cam, dir, sc);
+    const float a = sc.a, M = sc.M;
+    const float x = ry.s[0], y = ry.s[1], z = ry.s[2];
+    const float px = ry.s[3], py = ry.s[4], pz = ry.s[5];
+    const float E = -ry.pt, E2 = E * E;
+    const float L = z * px - x * pz;
+    const float r = ks_radius<float>(x, y, z, sc.aa);
+    const float ct = __fdividef(y, r);
+    const float st2 = fmaxf(1.0f - ct * ct, 1e-12f);
+    const float st = sqrtf(st2);
+    const float pth = __fdividef(ct, st) * (x * px + z * pz) - r * st * py;
+    const float Q = pth * pth + ct * ct * (__fdividef(L * L, st2) - a * a * E2);
+    const float K = (L - a * E) * (L - a * E) + Q;
+    const float B = a * (a * E - L);
+    const float c2 = 2.0f * E * B - K;
+    // Newton on R'(r) = 4 E^2 r^3 + 2 c2 r + 2 M K from the right of its largest root, where R'
+    // is increasing and convex: the iterates decrease monotonically onto the root
+    float rr = fmaxf(5.0f * M, sqrtf(__fdividef(fabsf(K), E2)));
+#pragma unroll 1
+    for (int it = 0; it < 16; ++it) {
+        const float d1 = 4.0f * E2 * rr * rr * rr + 2.0f * c2 * rr + 2.0f * M * K;
+        const float d2 = 12.0f * E2 * rr * rr + 2.0f * c2;
+        if (!(d2 > 0.0f)) break;
+        rr -= __fdividef(d1, d2);
+    }
+    const float r2 = rr * rr, r4 = r2 * r2;
+    const float Rm = E2 * r4 + c2 * r2 + 2.0f * M * K * rr + B * B - a * a * K;
+    return rr > sc.rh && fabsf(Rm) < kHotThreshold * E2 * r4;
+}
+
+// order[0], order[1]: marked / unmarked pixel counts; order[kOrderHeader + i]: pixel index
+// py * width + px of work unit i.  Units are written in warp-sized runs (a 16x2 patch of the
+// tile order, compacted): marked runs from the front, unmarked runs from the back.
+__device__ __forceinline__ void ordered_pixel(unsigned u, unsigned n, const unsigned* order, unsigned n_hot,
+                                              int W, int& px, int& py) {
+    const unsigned* list = order + kOrderHeader;
+    const unsigned idx = u < n_hot ? list[u] : list[n - 1u - (u - n_hot)];
+    py = (int)(idx / (unsigned)W);
+    px = (int)(idx - (unsigned)py * (unsigned)W);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) rank_pixels_kernel(const Scene sc, const Camera cam,
+                                                          unsigned* __restrict__ order) {
+    const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
+    const unsigned u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = u < n;
+    bool hot = false;
+    unsigned idx = 0;
+    if (valid) {
+        int px, py;
+        unit_to_pixel(u, sc.width, sc.height, px, py);
+        idx = (unsigned)py * (unsigned)sc.width + (unsigned)px;
+        float dir[3];
+        pixel_ray<MODE>(px, py, 0, sc, cam, dir);
+        hot = predicted_long(sc, cam, dir);
+    }
+    const unsigned hm = __ballot_sync(kFull, valid && hot);
+    const unsigned cm = __ballot_sync(kFull, valid && !hot);
+    unsigned hb = 0, cb = 0;
+    if (lane == 0) {
+        if (hm) hb = atomicAdd(order + 0, (unsigned)__popc(hm));
+        if (cm) cb = atomicAdd(order + 1, (unsigned)__popc(cm));
+    }
+    hb = __shfl_sync(kFull, hb, 0);
+    cb = __shfl_sync(kFull, cb, 0);
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned* list = order + kOrderHeader;
+    if (valid) {
+        if (hot)
+            list[hb + (unsigned)__popc(hm & lt)] = idx;
+        else
+            list[n - 1u - (cb + (unsigned)__popc(cm & lt))] = idx;
+    }
+}
+
+// Resident 256-thread blocks per SM asked of the compiler for the plain kernel: two for the
+// FP32 and mixed paths (at most 128 registers per thread, 16 warps per SM), one for FP64.
+template <class R> struct PlainMinBlocks { static constexpr int v = 2; };
+template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
+
+template <class R, int MODE, bool COUNT, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
+    trace_plain_kernel(const Scene sc, const Camera cam,
+                                                           float4* __restrict__ hdr,
+                                                           uint32_t* __restrict__ err,
+                                                           unsigned long long* __restrict__ ctr,
+                                                           float4* __restrict__ aux,
+                                                           const unsigned* __restrict__ order) {
+    int px, py;
+    if (order) {  // 1D launch over the ranked work units
+        const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
+        const unsigned u = blockIdx.x * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
+        if (u >= n) return;
+        ordered_pixel(u, n, order, order[0], sc.width, px, py);
+    } else {
+        px = blockIdx.x * blockDim.x + threadIdx.x;
+        py = blockIdx.y * blockDim.y + threadIdx.y;
+        if (px >= sc.width || py >= sc.height) return;
+    }
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    Tally total;
+    total.clear();
+    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total, aux);
+    const float fs = sc.final_scale;
+    hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+    if (COUNT) add_tally(ctr, (uint64_t)sc.spp, total);
+}
+
 // Persistent wavefront tracer.  A lane whose pixel is done takes a new one from the work
 // counter; lanes are refilled together once at least `refill_min` of the warp's lanes are idle
 // (or when the warp has nothing else to do), which trades idle lanes against how often the
@@ -125,10 +227,11 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
     trace_wavefront_kernel(const Scene sc, const Camera cam, float4* __restrict__ hdr,
                            uint32_t* __restrict__ err, unsigned* __restrict__ queue,
                            unsigned long long* __restrict__ ctr, float4* __restrict__ aux,
-                           int refill_min) {
+                           int refill_min, const unsigned* __restrict__ order) {
     const int lane = threadIdx.x & 31;
     const unsigned lane_lt = (1u << lane) - 1u;
     const unsigned n_units = (unsigned)sc.width * (unsigned)sc.height;
+    const unsigned n_hot = order ? order[0] : 0u;
     RayRun<R> ry;
     int px = 0, py = 0, smp = 0;
     float acc[3] = {0.0f, 0.0f, 0.0f};
@@ -153,7 +256,10 @@ __global__ void __launch_bounds__(kWavefrontBlock, MINB)
                 if (!active) {
                     const unsigned u = base + (unsigned)__popc(need & lane_lt);
                     if (u < n_units) {
-                        unit_to_pixel(u, sc.width, sc.height, px, py);
+                        if (order)
+                            ordered_pixel(u, n_units, order, n_hot, sc.width, px, py);
+                        else
+                            unit_to_pixel(u, sc.width, sc.height, px, py);
                         acc[0] = acc[1] = acc[2] = 0.0f;
                         // first sample with work; samples whose loop would not run add zero
                         for (smp = 0; smp < sc.spp; ++smp) {
@@ -213,20 +319,23 @@ template <> struct WaveDefaults<Mixed> { static constexpr int minb = 4; };
 
 template <class R, int MODE, bool COUNT>
 static cudaError_t launch_plain(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
-                                unsigned long long* ctr, float4* aux, int bx, int by, cudaStream_t st) {
+                                unsigned long long* ctr, float4* aux, int bx, int by, const unsigned* order,
+                                cudaStream_t st) {
     const dim3 block(bx, by);
-    const dim3 grid((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
+    const unsigned n = (unsigned)sc.width * (unsigned)sc.height, per = (unsigned)(bx * by);
+    const dim3 grid = order ? dim3((n + per - 1) / per)
+                            : dim3((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
     if (bx * by <= 256)
-        trace_plain_kernel<R, MODE, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux);
+        trace_plain_kernel<R, MODE, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
     else
-        trace_plain_kernel<R, MODE, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux);
+        trace_plain_kernel<R, MODE, COUNT, 1024><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
     return cudaGetLastError();
 }
 
 template <class R, int MODE, bool COUNT, int MINB>
 static cudaError_t launch_wave_minb(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
                                     unsigned* queue, unsigned long long* ctr, float4* aux, int refill,
-                                    cudaStream_t st) {
+                                    const unsigned* order, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -239,45 +348,52 @@ static cudaError_t launch_wave_minb(const Scene& sc, const Camera& cam, float4* 
     e = cudaMemsetAsync(queue, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
     trace_wavefront_kernel<R, MODE, COUNT, MINB>
-        <<<sms * per_sm, kWavefrontBlock, 0, st>>>(sc, cam, hdr, err, queue, ctr, aux, refill);
+        <<<sms * per_sm, kWavefrontBlock, 0, st>>>(sc, cam, hdr, err, queue, ctr, aux, refill, order);
     return cudaGetLastError();
 }
 
 template <class R, int MODE, bool COUNT>
 static cudaError_t launch_wave(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
                                unsigned* queue, unsigned long long* ctr, float4* aux, const Tuning& tn,
-                               cudaStream_t st) {
+                               const unsigned* order, cudaStream_t st) {
     const int refill = tn.refill_min < 1 ? 1 : (tn.refill_min > 32 ? 32 : tn.refill_min);
     if constexpr (std::is_same<R, float>::value && MODE == 0 && !COUNT) {
         switch (tn.blocks_per_sm) {
-            case 3: return launch_wave_minb<R, MODE, COUNT, 3>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
-            case 5: return launch_wave_minb<R, MODE, COUNT, 5>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
-            case 6: return launch_wave_minb<R, MODE, COUNT, 6>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
+            case 3: return launch_wave_minb<R, MODE, COUNT, 3>(sc, cam, hdr, err, queue, ctr, aux, refill, order, st);
+            case 5: return launch_wave_minb<R, MODE, COUNT, 5>(sc, cam, hdr, err, queue, ctr, aux, refill, order, st);
+            case 6: return launch_wave_minb<R, MODE, COUNT, 6>(sc, cam, hdr, err, queue, ctr, aux, refill, order, st);
             default: break;
         }
     }
-    return launch_wave_minb<R, MODE, COUNT, WaveDefaults<R>::minb>(sc, cam, hdr, err, queue, ctr, aux, refill, st);
+    return launch_wave_minb<R, MODE, COUNT, WaveDefaults<R>::minb>(sc, cam, hdr, err, queue, ctr, aux, refill, order, st);
 }
 
 template <class R, int MODE>
 static cudaError_t launch_typed(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
                                 uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
-                                const Tuning& tn, int bx, int by, cudaStream_t st) {
+                                const Tuning& tn, int bx, int by, unsigned* order, cudaStream_t st) {
+    if (order) {
+        const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
+        cudaError_t e = cudaMemsetAsync(order, 0, 2 * sizeof(unsigned), st);
+        if (e != cudaSuccess) return e;
+        rank_pixels_kernel<MODE><<<(n + 255) / 256, 256, 0, st>>>(sc, cam, order);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (schedule == 0)
-        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, aux, bx, by, st)
-                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, aux, bx, by, st);
-    return ctr ? launch_wave<R, MODE, true>(sc, cam, hdr, err, queue, ctr, aux, tn, st)
-               : launch_wave<R, MODE, false>(sc, cam, hdr, err, queue, ctr, aux, tn, st);
+        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, aux, bx, by, order, st)
+                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, aux, bx, by, order, st);
+    return ctr ? launch_wave<R, MODE, true>(sc, cam, hdr, err, queue, ctr, aux, tn, order, st)
+               : launch_wave<R, MODE, false>(sc, cam, hdr, err, queue, ctr, aux, tn, order, st);
 }
 
 cudaError_t launch_trace(const Scene& sc, const Camera& cam, int schedule, float4* hdr,
                          uint32_t* err, unsigned* queue, unsigned long long* ctr, float4* aux,
-                         const Tuning& tn, int bx, int by, cudaStream_t st) {
+                         const Tuning& tn, int bx, int by, unsigned* order, cudaStream_t st) {
     if (sc.width <= 0 || sc.height <= 0) return cudaSuccess;
-    if (sc.precision == 2) return launch_typed<double, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
-    if (sc.precision == 1) return launch_typed<Mixed, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
-    if (sc.mode == 1) return launch_typed<float, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
-    return launch_typed<float, 0>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, st);
+    if (sc.precision == 2) return launch_typed<double, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, order, st);
+    if (sc.precision == 1) return launch_typed<Mixed, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, order, st);
+    if (sc.mode == 1) return launch_typed<float, 1>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, order, st);
+    return launch_typed<float, 0>(sc, cam, schedule, hdr, err, queue, ctr, aux, tn, bx, by, order, st);
 }
 
 // ---- batched renders -----------------------------------------------------------------------

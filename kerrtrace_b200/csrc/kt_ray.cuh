@@ -192,25 +192,14 @@ __device__ __forceinline__ R crossing_root(R y0, R y1, R k1, R k3, R k4, R k5, R
     return t;
 }
 
-// Disk-plane crossing between prev and cur (cuda/kerr_trace.cuh:138-228): hit point on the
-// dense output, Novikov-Thorne disk test, redshift g, temperature from the disk LUT (with FBM
-// modulation), blackbody colour and alpha compositing.
+// Shading of a disk-plane hit `hit` (the state on the dense output at the crossing)
+// (cuda/kerr_trace.cuh:167-228): Novikov-Thorne disk test, redshift g, temperature from the disk
+// LUT (with FBM modulation), blackbody colour and alpha compositing into col / tau.
 template <class R, int MODE>
-__device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, const R* k1,
-                                               const R* k3, const R* k4, const R* k5,
-                                               const R* k6, const R* k7, R h, const Scene& sc,
-                                               uint32_t* err, Tally* tl) {
+__device__ __forceinline__ void shade_hit(const R* hit, R pt, R kt, float* col, float& tau, const Scene& sc,
+                                          uint32_t* err, Tally* tl) {
     using O = Ops<R>;
     const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
-    const R y0 = prev[1], y1 = ry.s[1];
-    const R dy = y0 - y1;
-    R t = dy != R(0) ? O::fdiv(y0, dy) : R(0.5);
-    t = O::minr(O::maxr(t, R(0)), R(1));
-    if (MODE == 1) t = crossing_root<R>(y0, y1, k1[1], k3[1], k4[1], k5[1], k6[1], k7[1], h, t);
-    R hit[6];
-#pragma unroll
-    for (int c = 0; c < 6; ++c)
-        hit[c] = dense_eval<R>(prev[c], ry.s[c], k1[c], k3[c], k4[c], k5[c], k6[c], k7[c], h, t);
     const R xh = hit[0], zh = hit[2], pxh = hit[3], pyh = hit[4], pzh = hit[5];
     R rh = ks_radius<R>(xh, R(0), zh, aa);
     const R r_in = (R)sc.disk_inner, r_out = (R)sc.disk_outer;
@@ -228,8 +217,8 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
     const R ldotxi = lx * zh - lz * xh;
     const R denH = r2h * r2h;
     const R Hk = M * rh * r2h * O::fdiv(R(1), denH);
-    const R L = (zh * pxh - xh * pzh) + R(2) * Hk * ldotxi * (ldotp + ry.kt);
-    const R energy = -ry.pt;
+    const R L = (zh * pxh - xh * pzh) + R(2) * Hk * ldotxi * (ldotp + kt);
+    const R energy = -pt;
     const R l_over_e = O::fdiv(L, energy);
     const R g = R(1) / (O::rsq(disc) * (R(1) - omega * l_over_e));
     const R span = r_out - r_in;
@@ -274,21 +263,42 @@ __device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, con
             const float luma = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
             const float luma_s = (float)((double)luma / sc.wl_step);
             const float alpha = 1.0f - __expf(-luma_s * 0.5f);
-            ry.col[0] += c.x * alpha * ry.tau;
-            ry.col[1] += c.y * alpha * ry.tau;
-            ry.col[2] += c.z * alpha * ry.tau;
-            ry.tau *= (1.0f - alpha);
+            col[0] += c.x * alpha * tau;
+            col[1] += c.y * alpha * tau;
+            col[2] += c.z * alpha * tau;
+            tau *= (1.0f - alpha);
         } else {
             const float3 c = blackbody_rgb_d(T, sc, err);
             const double luma = 0.2126 * (double)c.x + 0.7152 * (double)c.y + 0.0722 * (double)c.z;
             const double luma_s = luma / sc.wl_step;
             const double alpha = 1.0 - exp(-luma_s * 0.5);
-            ry.col[0] += (float)((double)c.x * alpha * (double)ry.tau);
-            ry.col[1] += (float)((double)c.y * alpha * (double)ry.tau);
-            ry.col[2] += (float)((double)c.z * alpha * (double)ry.tau);
-            ry.tau *= (float)(1.0 - alpha);
+            col[0] += (float)((double)c.x * alpha * (double)tau);
+            col[1] += (float)((double)c.y * alpha * (double)tau);
+            col[2] += (float)((double)c.z * alpha * (double)tau);
+            tau *= (float)(1.0 - alpha);
         }
     }
+}
+
+// Disk-plane crossing between prev and cur (cuda/kerr_trace.cuh:138-228): the hit point on the
+// dense output (reference semantics: the linear guess, kerr_trace.cuh:150-166; stated physics:
+// refined by the safeguarded Newton root), then shade_hit.
+template <class R, int MODE>
+__device__ __forceinline__ void shade_crossing(RayRun<R>& ry, const R* prev, const R* k1,
+                                               const R* k3, const R* k4, const R* k5,
+                                               const R* k6, const R* k7, R h, const Scene& sc,
+                                               uint32_t* err, Tally* tl) {
+    using O = Ops<R>;
+    const R y0 = prev[1], y1 = ry.s[1];
+    const R dy = y0 - y1;
+    R t = dy != R(0) ? O::fdiv(y0, dy) : R(0.5);
+    t = O::minr(O::maxr(t, R(0)), R(1));
+    if (MODE == 1) t = crossing_root<R>(y0, y1, k1[1], k3[1], k4[1], k5[1], k6[1], k7[1], h, t);
+    R hit[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        hit[c] = dense_eval<R>(prev[c], ry.s[c], k1[c], k3[c], k4[c], k5[c], k6[c], k7[c], h, t);
+    shade_hit<R, MODE>(hit, ry.pt, ry.kt, ry.col, ry.tau, sc, err, tl);
 }
 
 // One DP5(4) attempt; on the last attempt of a step, the commit and the per-step tests.
@@ -395,12 +405,16 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
 // Mixed precision (stated physics only).  The state is a float pair: hi carries every FP32
 // computation (right-hand sides, stages, tests), lo the part of an FP64 value below hi.
 // Outside the photon zone (Kerr-Schild radius of the step start >= sc.zone_r, 1.5 x the
-// retrograde photon-orbit radius) lo is 0 and the step is exactly the FP32 step.  Inside it the
-// state update x + h sum b_i k_i and the embedded error norm run in FP64 on hi + lo, every
-// accepted step renormalises p onto the null cone in FP64, and the result is split back into
-// hi and lo.  The crossing root and the shading run in FP64.
+// retrograde photon-orbit radius, which contains the horizon) lo is 0 and the step is exactly
+// the FP32 step.  Inside it the state update x + h sum b_i k_i runs in FP64 on hi + lo, every
+// kRenormEvery-th accepted step renormalises p onto the null cone in FP64, and the result is
+// split back into hi and lo.  The embedded error norm runs in FP64 when the tolerance is below
+// 3e-7 (sc.zone_err64): the FP32 stage sum carries an absolute error of about
+// 6e-9 h |k|, under 1% of the tolerance scale above that.  A crossing is located in FP32, its
+// root refined by FP64 Newton steps on the hi + lo dense output, and the hit shaded in FP32.
 // =========================================================================================
 struct Mixed {};
+constexpr int kRenormEvery = 8;
 
 template <>
 struct RayRun<Mixed> {
@@ -415,27 +429,49 @@ struct RayRun<Mixed> {
     bool have_k1, zone;
 };
 
-// Rescales p so that H(x, p) = 0 exactly: with H = (|p|^2 - pt^2 - 2 Hk (l.p - pt)^2) / 2 and
-// p -> lambda p, lambda solves (|p|^2 - 2 Hk (l.p)^2) lambda^2 + 4 Hk pt (l.p) lambda
-// - pt^2 (1 + 2 Hk) = 0; the root next to 1 is taken (no change when none is within 1e-3).
+// FP64 reciprocal and reciprocal square root without the long-latency IEEE sequences: the FP32
+// hardware approximation as the seed, then two Newton-Raphson steps (r <- r + r (1 - x r) and
+// y <- y + y (1/2 - x y^2 / 2)); each step doubles the correct bits, 22 -> 44 -> beyond 53.
+// Valid for |x| within the FP32 range, which holds for every quantity they are used on here.
+__device__ __forceinline__ double rcp_nr(double x) {
+    double r = (double)__fdividef(1.0f, (float)x);
+    r = fma(r, fma(-x, r, 1.0), r);
+    return fma(r, fma(-x, r, 1.0), r);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y = (double)rsqrtf((float)x);
+    const double hx = 0.5 * x;
+    y = fma(y, fma(-hx * y, y, 0.5), y);
+    return fma(y, fma(-hx * y, y, 0.5), y);
+}
+
+// Rescales p onto the null cone: with H(p) = (|p|^2 - pt^2 - 2 Hk (l.p - pt)^2) / 2 and
+// p -> lambda p, H is A lambda^2 + B lambda + C with A = |p|^2 - 2 Hk (l.p)^2,
+// B = 4 Hk pt (l.p), C = -pt^2 (1 + 2 Hk).  One Newton step from lambda = 1,
+// lambda = 1 - (A + B + C) / (2A + B), removes the drift of an accurate step (the residual is
+// quadratic in it).  No change unless the correction is below 1e-3.
 __device__ __forceinline__ void null_renormalise(double* s, double pt, const Scene& sc) {
     const double a = sc.a_d, aa = sc.aa_d, M = sc.M_d;
     const double x = s[0], y = s[1], z = s[2];
-    const double r = ks_radius<double>(x, y, z, aa);
-    const double r2 = r * r, D = r2 + aa;
-    const double lx = (r * x - a * z) / D, ly = y / r, lz = (r * z + a * x) / D;
-    const double Hk = M * r2 * r / (r2 * r2 + aa * y * y);
+    const double rho2 = x * x + y * y + z * z;
+    const double u = rho2 - aa;
+    const double q = u * u + 4.0 * aa * y * y;
+    const double r2 = 0.5 * (u + q * rsqrt_nr(q));
+    const double inv_r = rsqrt_nr(r2);
+    const double r = r2 * inv_r;
+    const double inv_D = rcp_nr(r2 + aa);
+    const double lx = (r * x - a * z) * inv_D, ly = y * inv_r, lz = (r * z + a * x) * inv_D;
+    const double Hk = M * r2 * r * rcp_nr(r2 * r2 + aa * y * y);
     const double lp = lx * s[3] + ly * s[4] + lz * s[5];
     const double pp = s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
     const double A = pp - 2.0 * Hk * lp * lp;
     const double B = 4.0 * Hk * pt * lp;
     const double Cq = -pt * pt * (1.0 + 2.0 * Hk);
-    const double disc = B * B - 4.0 * A * Cq;
-    if (!(A > 0.0) || !(disc >= 0.0)) return;
-    const double sq = sqrt(disc);
-    const double l1 = (-B + sq) / (2.0 * A), l2 = (-B - sq) / (2.0 * A);
-    const double lam = fabs(l1 - 1.0) < fabs(l2 - 1.0) ? l1 : l2;
-    if (!(fabs(lam - 1.0) < 1e-3)) return;
+    const double den = 2.0 * A + B;
+    if (!(den != 0.0)) return;
+    const double dl = -(A + B + Cq) * rcp_nr(den);
+    if (!(fabs(dl) < 1e-3)) return;
+    const double lam = 1.0 + dl;
     s[3] *= lam;
     s[4] *= lam;
     s[5] *= lam;
@@ -465,34 +501,32 @@ __device__ __forceinline__ bool ray_start_mixed(RayRun<Mixed>& ry, const Camera&
     return run;
 }
 
-// Disk crossing of a mixed-precision step, shaded in FP64 from the hi/lo states.  Kept out of
-// line: it runs on few steps and would otherwise raise the register count of the whole loop.
-// ks rows: k1, k3, k4, k5, k6, k7, lo of the step start.
+// Disk crossing of a mixed-precision step.  Kept out of line: it runs on few steps and would
+// otherwise raise the register count of the whole loop.  ks rows: k1, k3, k4, k5, k6, k7, lo
+// of the step start; tc: the FP32 root.  Two FP64 Newton steps on the hi + lo dense output take
+// the root to FP64 accuracy; the hit is then shaded in FP32.
 static __device__ __noinline__ void shade_mixed(RayRun<Mixed>& ry, const float* prev, const float (*ks)[6], float h,
-                                         const Scene& sc, uint32_t* err, Tally* tl) {
-    RayRun<double> dr;
-    double pd[6], k1d[6], k3d[6], k4d[6], k5d[6], k6d[6], k7d[6];
+                                                float tc, const Scene& sc, uint32_t* err, Tally* tl) {
+    double y0[6], y1[6];
     for (int c = 0; c < 6; ++c) {
-        pd[c] = (double)prev[c] + (double)ks[6][c];
-        dr.s[c] = (double)ry.s[c] + (double)ry.lo[c];
-        k1d[c] = ks[0][c];
-        k3d[c] = ks[1][c];
-        k4d[c] = ks[2][c];
-        k5d[c] = ks[3][c];
-        k6d[c] = ks[4][c];
-        k7d[c] = ks[5][c];
+        y0[c] = (double)prev[c] + (double)ks[6][c];
+        y1[c] = (double)ry.s[c] + (double)ry.lo[c];
     }
-    dr.pt = ry.pt;
-    dr.kt = ry.kt;
-    dr.col[0] = ry.col[0];
-    dr.col[1] = ry.col[1];
-    dr.col[2] = ry.col[2];
-    dr.tau = ry.tau;
-    shade_crossing<double, 1>(dr, pd, k1d, k3d, k4d, k5d, k6d, k7d, (double)h, sc, err, tl);
-    ry.col[0] = dr.col[0];
-    ry.col[1] = dr.col[1];
-    ry.col[2] = dr.col[2];
-    ry.tau = dr.tau;
+    const double hd = (double)h;
+    double t = (double)tc;
+    for (int it = 0; it < 2; ++it) {
+        const double yt = dense_eval<double>(y0[1], y1[1], ks[0][1], ks[1][1], ks[2][1], ks[3][1], ks[4][1],
+                                             ks[5][1], hd, t);
+        const double dyt = dense_slope<double>(y0[1], y1[1], ks[0][1], ks[1][1], ks[2][1], ks[3][1], ks[4][1],
+                                               ks[5][1], hd, t);
+        if (!(fabs(dyt) > 0.0)) break;
+        t = fmin(fmax(t - yt / dyt, 0.0), 1.0);
+    }
+    float hit[6];
+    for (int c = 0; c < 6; ++c)
+        hit[c] = (float)dense_eval<double>(y0[c], y1[c], ks[0][c], ks[1][c], ks[2][c], ks[3][c], ks[4][c],
+                                           ks[5][c], hd, t);
+    shade_hit<float, 1>(hit, (float)ry.pt, (float)ry.kt, ry.col, ry.tau, sc, err, tl);
 }
 
 template <int MODE, bool COUNT>
@@ -550,22 +584,23 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
     }
     hamilton_rhs<float, EXACT>(nx, pt, a, aa, M, k7);
     float errv;
-    if (ry.zone) {
+    if (COUNT && ry.zone) tl.fp64++;
+    if (ry.zone && sc.zone_err64) {
         double em = 0.0;
         bool any = false;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             const double e = (double)h * (CD::e1 * (double)k1[c] + CD::e3 * (double)k3[c] + CD::e4 * (double)k4[c] +
                                           CD::e5 * (double)k5[c] + CD::e6 * (double)k6[c] + CD::e7 * (double)k7[c]);
-            const double sd = (double)s[c] + (double)ry.lo[c];
-            const double ec = fabs(e) / ((double)ry.tol * fmax(fabs(sd), 1.0));
+            // the FP64 part is the stage sum, where the terms cancel; the scaling is FP32
+            const float scale = ry.tol * O::maxr(O::absr(s[c]), 1.0f);
+            const double ec = fabs(e) * (double)__fdividef(1.0f, scale);
             if (ec == ec) {
                 em = any ? fmax(em, ec) : ec;
                 any = true;
             }
         }
         errv = any ? (float)em : __int_as_float(0x7fffffff);
-        if (COUNT) tl.fp64++;
     } else {
         float e[6];
 #pragma unroll
@@ -595,7 +630,7 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
         double nd[6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) nd[c] = ((double)prev[c] + (double)prev_lo[c]) + (double)h * (double)inc[c];
-        if (ok) null_renormalise(nd, ry.pt, sc);
+        if (ok && ry.step % kRenormEvery == 0) null_renormalise(nd, ry.pt, sc);
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             ry.s[c] = (float)nd[c];
@@ -613,7 +648,21 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
     }
     const float r_now = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa);
     if (inside_horizon<float>(r_now, sc)) return true;
+    bool near_disk = false;
+    float tc = 0.5f;
     if ((prev[1] < 0.0f && ry.s[1] >= 0.0f) || (prev[1] > 0.0f && ry.s[1] <= 0.0f)) {
+        // FP32 estimate of the hit radius first: the FP64 root and shading only run for
+        // crossings that can land on the disk (1e-3 margin on both radii)
+        const float dyc = prev[1] - ry.s[1];
+        tc = dyc != 0.0f ? __fdividef(prev[1], dyc) : 0.5f;
+        tc = fminf(fmaxf(tc, 0.0f), 1.0f);
+        tc = crossing_root<float>(prev[1], ry.s[1], k1[1], k3[1], k4[1], k5[1], k6[1], k7[1], h, tc);
+        const float xc = dense_eval<float>(prev[0], ry.s[0], k1[0], k3[0], k4[0], k5[0], k6[0], k7[0], h, tc);
+        const float zc = dense_eval<float>(prev[2], ry.s[2], k1[2], k3[2], k4[2], k5[2], k6[2], k7[2], h, tc);
+        const float rc = ks_radius<float>(xc, 0.0f, zc, aa);
+        near_disk = rc >= sc.disk_inner * 0.999f && rc <= sc.disk_outer * 1.001f;
+    }
+    if (near_disk) {
         float ks[7][6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
@@ -625,7 +674,7 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
             ks[5][c] = k7[c];
             ks[6][c] = prev_lo[c];
         }
-        shade_mixed(ry, prev, ks, h, sc, err, COUNT ? &tl : nullptr);
+        shade_mixed(ry, prev, ks, h, tc, sc, err, COUNT ? &tl : nullptr);
     }
     if (ok) {
 #pragma unroll

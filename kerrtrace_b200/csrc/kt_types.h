@@ -45,6 +45,7 @@ struct Scene {
     unsigned noise_seed;
     float noise_phase;
     float zone_r;        // mixed precision: FP64 update below this Kerr-Schild radius
+    int zone_err64;      // mixed precision: FP64 error norm in the zone (tolerance below 3e-7)
     float spec_tol_floor;// stated physics: tolerance never drops below base_tol * this
     int width, height;
 };

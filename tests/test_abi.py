@@ -33,7 +33,7 @@ def test_every_declared_symbol_is_exported(kt):
 
 def test_library_loads_and_versions(kt):
     L = kt.lib()
-    assert L.kt_abi_version() == 1
+    assert L.kt_abi_version() == 2
     assert L.kt_status_str(kt.KT_ERR_LUT_OVERFLOW).decode().startswith("colour temperature")
 
 

@@ -113,3 +113,39 @@ def test_block_dims(cuda):
         c.block_dim[0], c.block_dim[1] = bx, by
         out, _, _, _ = run_ours(cuda, c, cam, kt.SCHED_PLAIN)
         assert np.array_equal(out.view(np.uint32), base.view(np.uint32)), (bx, by)
+
+
+ORDER_CASES = [("c1", 0, 0, (100, 60)), ("t1", 0, 0, None), ("t2", 1, 0, None), ("c2", 1, 0, (320, 180)),
+               ("t1", 1, 1, None), ("t2", 1, 2, None)]
+
+
+@pytest.mark.parametrize("name,mode,prec,size", ORDER_CASES)
+@pytest.mark.parametrize("schedule", [kt.SCHED_PLAIN, kt.SCHED_WAVEFRONT])
+def test_long_first_order_is_bit_identical(cuda, name, mode, prec, size, schedule):
+    """The long-rays-first order writes every pixel once (NaN-filled output, alpha 1 everywhere
+    after the trace) with the bits and the work totals of the tile order (partial tiles and a
+    pixel count that is not a multiple of 32 included)."""
+    cfg, cam = workloads.scene(name)
+    if size:
+        cfg = workloads.scaled(cfg, *size)
+    cfg.mode, cfg.precision = mode, prec
+    ctx = kt.Context(cfg)
+    ctx.set_tuning(schedule=schedule, block_x=8, block_y=8, order=kt.ORDER_TILES)
+    base, eb, sb, _ = run_ours(cuda, cfg, cam, schedule, counted=True, ctx=ctx)
+    ctx.set_tuning(schedule=schedule, block_x=8, block_y=8, order=kt.ORDER_LONG_FIRST)
+    assert ctx.tuning().order == kt.ORDER_LONG_FIRST
+    n = cfg.width * cfg.height
+    for counted in (False, True):
+        hdr = cuda.full((n, 4), float("nan"), device="cuda")
+        err = cuda.zeros(2, dtype=cuda.int32, device="cuda")
+        if counted:
+            st = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), 0, schedule)
+            for f in ("rays", "steps", "attempts", "rhs_evals", "frozen_rays", "fp64_steps"):
+                assert getattr(st, f) == getattr(sb, f), f
+        else:
+            ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), 0, kt.SCHED_AUTO)
+        cuda.cuda.synchronize()
+        out = hdr.cpu().numpy()
+        assert np.all(out[:, 3] == 1.0)
+        assert np.array_equal(out.view(np.uint32), base.view(np.uint32))
+        assert np.array_equal(err.cpu().numpy().view(np.uint32), eb)

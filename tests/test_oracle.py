@@ -116,6 +116,40 @@ def test_null_initialisation_and_conservation():
         assert abs(hamiltonian(s, pt, a, 1.0)) < 1e-9
 
 
+def kerr_constants(st, pt, a):
+    """E = -p_t, the angular momentum about the spin axis (y) and the Carter constant of a
+    Kerr-Schild Cartesian state; p_theta comes from the spheroidal coordinates of the point,
+    X + iY = (r + i a) e^{i phi} sin(theta), Z = r cos(theta) with (X, Y, Z) = (x, -z, y).  The
+    trace kernels' long-ray predictor uses these expressions."""
+    x, y, z, px, py, pz = st
+    r = ks_r(x, y, z, a)
+    E = -pt
+    L = z * px - x * pz
+    ct = y / r
+    s2 = 1.0 - ct * ct
+    pth = ct / math.sqrt(s2) * (x * px + z * pz) - r * math.sqrt(s2) * py
+    Q = pth * pth + ct * ct * (L * L / s2 - a * a * E * E)
+    return E, L, Q
+
+
+@pytest.mark.parametrize("a", [0.0, 0.9, -0.7])
+@pytest.mark.parametrize("d", [[-1.0, -0.12, 0.35], [-1.0, 0.3, 0.3]])
+def test_kerr_constants_of_motion_are_conserved(a, d):
+    """L and Q stay constant along the oracle's (exact-gradient) integration of a ray that
+    passes the hole within 11 M, which pins both the expressions and the oracle's dynamics."""
+    st, pt = null_init([20.0, 3.0, 2.0], d, a)
+    E0, L0, Q0 = kerr_constants(st, pt, a)
+    s = st.copy()
+    r_min = 1e9
+    for _ in range(600):
+        s, _ = dp5(s, pt, a, 1.0, 0.05)
+        r_min = min(r_min, ks_r(s[0], s[1], s[2], a))
+    E1, L1, Q1 = kerr_constants(s, pt, a)
+    assert r_min < 11.0 and ks_r(s[0], s[1], s[2], a) > r_min + 2.0  # passed the hole
+    assert abs(L1 - L0) < 1e-10 * max(1.0, abs(L0))
+    assert abs(Q1 - Q0) < 1e-10 * max(1.0, abs(Q0))
+
+
 def test_dp5_orders():
     """Local error of the 5th-order update is O(h^6); the embedded estimate is O(h^5)."""
     st, pt = null_init([12.0, 2.0, 1.0], [-1.0, 0.2, 0.3], 0.6)
