@@ -241,8 +241,9 @@ kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, f
  * 0x00RRGGBB.  bloom may be NULL when bloom is inactive. */
 kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const float* bloom,
                           uint32_t* image_out);
-/* Both post passes in one kernel (no bloom buffer round trip); same output bits as
- * kt_bloom_horizontal followed by kt_post_process. */
+/* Both post passes through the context's own bloom buffer (allocated with the context when
+ * bloom is active): same output bits as kt_bloom_horizontal followed by kt_post_process.  Calls
+ * on one context must not overlap in time (they share that buffer). */
 kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_t* image_out);
 
 /* ---- batched renders (many scenes / cameras in one launch) -------------------------------- */

@@ -435,6 +435,7 @@ struct kt_context {
     ktd::Tuning tuning;                     // persistent-tracer launch shape
     unsigned long long* counters = nullptr; // 6 x u64 for the counting launches
     unsigned* order = nullptr;              // pixel order (allocated when a tuning asks for it)
+    float4* bloom_scratch = nullptr;        // kt_post_fused's bloom buffer (when bloom is active)
     int block_x = 16, block_y = 16;
 };
 
@@ -454,6 +455,7 @@ void destroy_ctx(kt_context* c) {
     cudaFree(c->queue);
     cudaFree(c->counters);
     cudaFree(c->order);
+    cudaFree(c->bloom_scratch);
     cudaSetDevice(prev);
     delete c;
 }
@@ -637,6 +639,8 @@ kt_status create_impl(const kt_config* cfg, int device, const float* bb_in, cons
         (e = cudaMalloc(&c->disk_lut_dev, disk.size() * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&c->queue, 64)) != cudaSuccess ||
         (e = cudaMalloc(&c->counters, 8 * sizeof(unsigned long long))) != cudaSuccess ||
+        (c->post.active &&
+         (e = cudaMalloc(&c->bloom_scratch, (size_t)cfg->width * cfg->height * sizeof(float4))) != cudaSuccess) ||
         (e = cudaMemcpy(c->bb_lut_dev, bb.data(), bb.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(c->disk_lut_dev, disk.data(), disk.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
         return step(cuda_fail(e, "context allocation"));
@@ -808,7 +812,7 @@ kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_
     if (!ctx || !hdr || !image_out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
     DeviceGuard g(ctx->device);
     const cudaError_t e = ktd::launch_post_fused(ctx->post, reinterpret_cast<const float4*>(hdr), image_out,
-                                                 (cudaStream_t)stream);
+                                                 ctx->bloom_scratch, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "fused post launch");
     return KT_OK;
 }

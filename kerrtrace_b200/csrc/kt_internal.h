@@ -67,7 +67,8 @@ cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, flo
                                     cudaStream_t stream);
 cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const float4* bloom,
                                 uint32_t* image, cudaStream_t stream);
-cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image,
+// Both post passes; scratch: a width x height float4 bloom buffer (unused when bloom is off).
+cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image, float4* scratch,
                               cudaStream_t stream);
 
 }  // namespace ktd

@@ -11,13 +11,12 @@
 //                           pulls a new one from a device work counter (warp-aggregated atomics)
 //                           as soon as its rays are done, so long rays never idle a whole warp.
 // Post kernels (replace bloom_horizontal / post_process, cuda/kernel.cu:144-251):
-//   bloom_h_kernel          horizontal normalised Gaussian from a shared-memory row segment
-//   post_v_kernel           vertical Gaussian from a shared-memory column tile + composite,
-//                           ACES, sRGB OETF, 0x00RRGGBB pack
-//   post_fused_kernel       both passes in one kernel, the horizontal result kept in shared
-//                           memory (no bloom buffer round trip through HBM)
-// All three post paths produce the reference's bits: same tap order, same weights, same
-// division and tone-map expressions.
+//   bloom_h_kernel          horizontal normalised Gaussian, register-blocked over staged rows
+//   post_v_kernel           vertical Gaussian streamed from the bloom buffer + composite, ACES,
+//                           sRGB OETF, 0x00RRGGBB pack
+//   tonemap_kernel          tone map alone (bloom inactive)
+// kt_post_fused runs both passes over a bloom buffer that the context owns.  The post kernels
+// produce the reference's bits: same tap order, weights, division and tone-map expressions.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -472,177 +471,218 @@ __device__ __forceinline__ float4 bloom_source(float4 c, const PostParams& pp) {
     return make_float4(c.x * k, c.y * k, c.z * k, c.w);
 }
 
-constexpr int kRowSeg = 256;  // bloom_h: pixels per block
+// ---- separable Gaussian, register-blocked ------------------------------------------------
+// Each thread makes kBJ consecutive outputs along the blur direction from one stream of
+// kBJ + 2R source values: value k feeds output j with weight w[k - j] (tap i = k - j - R), so
+// every output still accumulates its taps in increasing i, the order of the reference's loop
+// (cuda/kernel.cu:156-166, 199-209), with the same contracted multiply-adds, and gets the same
+// bits.  A source value is read once per kBJ outputs instead of once per output.  The weight
+// sum of an output (its in-image weights, added in the same order) depends only on its position
+// and is computed once per block.  Chunks whose taps all lie inside the image run the head /
+// middle / tail loop; chunks at the border run the reference's per-output loop.
+constexpr int kBJ = 8;
 
-// Horizontal pass: one block per 256-pixel row segment, the segment and its halo staged once.
-__global__ void __launch_bounds__(kRowSeg) bloom_h_kernel(const PostParams pp,
-                                                          const float4* __restrict__ hdr,
-                                                          float4* __restrict__ bloom) {
-    extern __shared__ float4 smem4[];
-    const int R = pp.radius;
-    float* w = reinterpret_cast<float*>(smem4 + kRowSeg + 2 * R);
-    const int y = blockIdx.y;
-    const int x0 = blockIdx.x * kRowSeg;
-    for (int i = threadIdx.x; i <= 2 * R; i += blockDim.x) w[i] = tap_weight(i - R, pp.sigma);
-    for (int j = threadIdx.x; j < kRowSeg + 2 * R; j += blockDim.x) {
-        const int gx = x0 - R + j;
-        smem4[j] = (gx >= 0 && gx < pp.width) ? bloom_source(__ldg(hdr + (size_t)y * pp.width + gx), pp)
-                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+template <class Load>
+__device__ __forceinline__ void blur_interior(const Load& load, const float* w, int R, float (&acc)[kBJ][3]) {
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0f;
+    // head: value k (< kBJ - 1) feeds outputs 0..k
+#pragma unroll
+    for (int k = 0; k < kBJ - 1; ++k) {
+        const float4 v = load(k);
+#pragma unroll
+        for (int j = 0; j <= k; ++j) {
+            const float wi = w[k - j];
+            acc[j][0] += v.x * wi;
+            acc[j][1] += v.y * wi;
+            acc[j][2] += v.z * wi;
+        }
     }
-    __syncthreads();
-    const int x = x0 + threadIdx.x;
-    if (x >= pp.width) return;
-    float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
-    for (int i = -R; i <= R; ++i) {
-        const int sx = x + i;
-        if (sx < 0 || sx >= pp.width) continue;
-        const float wi = w[i + R];
-        const float4 c = smem4[threadIdx.x + R + i];
-        ax += c.x * wi;
-        ay += c.y * wi;
-        az += c.z * wi;
-        ws += wi;
+    // middle: every output; wr[j] = w[k - j] slides with k (w has a zero at index 2R + 1)
+    float wr[kBJ];
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j) wr[j] = w[kBJ - 1 - j];
+#pragma unroll 4
+    for (int k = kBJ - 1; k <= 2 * R; ++k) {
+        const float4 v = load(k);
+#pragma unroll
+        for (int j = 0; j < kBJ; ++j) {
+            acc[j][0] += v.x * wr[j];
+            acc[j][1] += v.y * wr[j];
+            acc[j][2] += v.z * wr[j];
+        }
+#pragma unroll
+        for (int j = kBJ - 1; j > 0; --j) wr[j] = wr[j - 1];
+        wr[0] = w[k + 1];
     }
-    if (ws > 0.0f) {
-        ax /= ws;
-        ay /= ws;
-        az /= ws;
+    // tail: value 2R + t feeds outputs t..kBJ-1
+#pragma unroll
+    for (int t = 1; t < kBJ; ++t) {
+        const float4 v = load(2 * R + t);
+#pragma unroll
+        for (int j = t; j < kBJ; ++j) {
+            const float wi = w[2 * R + t - j];
+            acc[j][0] += v.x * wi;
+            acc[j][1] += v.y * wi;
+            acc[j][2] += v.z * wi;
+        }
     }
-    bloom[(size_t)y * pp.width + x] = make_float4(ax, ay, az, 0.0f);
 }
 
-constexpr int kPostTX = 32, kPostTY = 8;
-
-// Vertical pass + composite + tone map: a 32-column strip of (8 + 2R) bloom rows in shared memory.
-__global__ void __launch_bounds__(kPostTX * kPostTY) post_v_kernel(const PostParams pp,
-                                                                    const float4* __restrict__ hdr,
-                                                                    const float4* __restrict__ bloom,
-                                                                    uint32_t* __restrict__ image) {
-    extern __shared__ float4 smem4[];
-    const int R = pp.active ? pp.radius : 0;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x = blockIdx.x * kPostTX + tx;
-    const int y = blockIdx.y * kPostTY + ty;
-    float* w = reinterpret_cast<float*>(smem4 + (kPostTY + 2 * R) * kPostTX);
-    if (pp.active) {
-        const int tid = ty * kPostTX + tx;
-        for (int i = tid; i <= 2 * R; i += kPostTX * kPostTY) w[i] = tap_weight(i - R, pp.sigma);
-        for (int row = ty; row < kPostTY + 2 * R; row += kPostTY) {
-            const int gy = blockIdx.y * kPostTY + row - R;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (x < pp.width && gy >= 0 && gy < pp.height) v = __ldg(bloom + (size_t)gy * pp.width + x);
-            smem4[row * kPostTX + tx] = v;
-        }
-        __syncthreads();
-    }
-    if (x >= pp.width || y >= pp.height) return;
-    const size_t idx = (size_t)y * pp.width + x;
-    const float4 base = __ldg(hdr + idx);
-    float fr = base.x, fg = base.y, fb = base.z;
-    if (pp.active) {
-        float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+// Border chunk: the reference's loop per output, out-of-image taps skipped.  pos0 = position of
+// output 0 along the blur, n = image extent along it; load(k) is only called for in-image taps.
+template <class Load>
+__device__ __forceinline__ void blur_edge(const Load& load, const float* w, int R, int pos0, int n,
+                                          float (&acc)[kBJ][3]) {
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j) {
+        float ax = 0.0f, ay = 0.0f, az = 0.0f;
         for (int i = -R; i <= R; ++i) {
-            const int sy = y + i;
-            if (sy < 0 || sy >= pp.height) continue;
+            const int sp = pos0 + j + i;
+            if (sp < 0 || sp >= n) continue;
             const float wi = w[i + R];
-            const float4 c = smem4[(ty + R + i) * kPostTX + tx];
+            const float4 c = load(j + i + R);
             ax += c.x * wi;
             ay += c.y * wi;
             az += c.z * wi;
-            ws += wi;
         }
+        acc[j][0] = ax;
+        acc[j][1] = ay;
+        acc[j][2] = az;
+    }
+}
+
+// Sum of the in-image tap weights of the output at `pos` (n = extent), in tap order.
+__device__ __forceinline__ float weight_sum(int pos, int n, const float* w, int R) {
+    float ws = 0.0f;
+    for (int i = -R; i <= R; ++i) {
+        const int sp = pos + i;
+        if (sp < 0 || sp >= n) continue;
+        ws += w[i + R];
+    }
+    return ws;
+}
+
+__device__ __forceinline__ void load_weights(float* w, int R, float sigma, int tid, int nthreads) {
+    for (int i = tid; i <= 2 * R + 1; i += nthreads) w[i] = i <= 2 * R ? tap_weight(i - R, sigma) : 0.0f;
+}
+
+// Horizontal pass (bloom_horizontal, cuda/kernel.cu:144-173): a block makes a 32-row x 64-column
+// tile.  Lane = row, warp = a kBJ-column chunk, so every tap test is uniform across the warp.
+// The 32 source rows (64 + 2R columns) are staged with coalesced loads at an odd float4 row
+// stride (conflict-free column reads); the results go back through the same shared memory for
+// coalesced stores.
+constexpr int kHRows = 32, kHWarps = 8, kHCols = kHWarps * kBJ;
+
+__host__ __device__ constexpr int bloom_h_stride(int R) { return (kHCols + 2 * R) | 1; }
+
+__global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostParams pp,
+                                                                    const float4* __restrict__ hdr,
+                                                                    float4* __restrict__ bloom) {
+    extern __shared__ float4 smem4[];
+    const int R = pp.radius;
+    const int segw = kHCols + 2 * R, stride = bloom_h_stride(R);
+    float4* stage = smem4;                                             // kHRows x stride
+    float* w = reinterpret_cast<float*>(stage + kHRows * stride);      // 2R + 2
+    float* wsum = w + 2 * R + 2;                                       // kHCols
+    const int x0 = blockIdx.x * kHCols, y0 = blockIdx.y * kHRows;
+    const int tid = threadIdx.x;
+    load_weights(w, R, pp.sigma, tid, blockDim.x);
+    for (int j = tid; j < kHRows * segw; j += blockDim.x) {
+        const int r = j / segw, c = j - r * segw;
+        const int gy = y0 + r, gx = x0 - R + c;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gy < pp.height && gx >= 0 && gx < pp.width) v = bloom_source(__ldg(hdr + (size_t)gy * pp.width + gx), pp);
+        stage[r * stride + c] = v;
+    }
+    __syncthreads();
+    if (tid < kHCols) wsum[tid] = weight_sum(x0 + tid, pp.width, w, R);
+    const int lane = tid & 31, cb = (tid >> 5) * kBJ;
+    const float4* row = stage + lane * stride + cb;
+    auto load = [row](int k) { return row[k]; };
+    float acc[kBJ][3];
+    const int xs = x0 + cb;
+    if (2 * R >= kBJ - 1 && xs - R >= 0 && xs + kBJ - 1 + R < pp.width)
+        blur_interior(load, w, R, acc);
+    else
+        blur_edge(load, w, R, xs, pp.width, acc);
+    __syncthreads();  // staged sources no longer read; wsum written
+    constexpr int ostride = kHCols + 1;
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j) {
+        const float ws = wsum[cb + j];
+        float ax = acc[j][0], ay = acc[j][1], az = acc[j][2];
         if (ws > 0.0f) {
             ax /= ws;
             ay /= ws;
             az /= ws;
         }
-        fr += ax * pp.intensity;
-        fg += ay * pp.intensity;
-        fb += az * pp.intensity;
+        stage[lane * ostride + cb + j] = make_float4(ax, ay, az, 0.0f);
     }
-    image[idx] = tone_pack(fr, fg, fb);
+    __syncthreads();
+    for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
+        const int r = j / kHCols, c = j - r * kHCols;
+        const int gy = y0 + r, gx = x0 + c;
+        if (gy < pp.height && gx < pp.width) bloom[(size_t)gy * pp.width + gx] = stage[r * ostride + c];
+    }
 }
 
-// Fused post: tile of 64 x 32 output pixels.  Phase 1 computes the horizontal blur of the
-// (32 + 2R) source rows of the tile into shared memory, staging 8 HDR rows (with their
-// horizontal halo) at a time; phase 2 runs the vertical blur, composite and tone map.
-constexpr int kFuseTX = 64, kFuseTY = 32, kFuseChunk = 8, kFuseThreads = 256;
+// Vertical pass + composite + ACES + sRGB + pack (post_process, cuda/kernel.cu:175-251): a block
+// makes a 64-column x 32-row tile; warp w covers 32 columns ((w & 1) * 32) and kBJ rows
+// ((w >> 1) * kBJ); each thread streams its column of the bloom buffer with coalesced loads.
+constexpr int kVCols = 64, kVRows = 32, kVThreads = 256;
 
-__global__ void __launch_bounds__(kFuseThreads) post_fused_kernel(const PostParams pp,
-                                                                   const float4* __restrict__ hdr,
-                                                                   uint32_t* __restrict__ image) {
-    extern __shared__ float4 smem4[];
-    const int R = pp.radius;
-    const int segw = kFuseTX + 2 * R;
-    float4* stage = smem4;                                       // kFuseChunk x segw
-    float* hb = reinterpret_cast<float*>(stage + kFuseChunk * segw);  // (TY+2R) x TX x 3
-    float* w = hb + (kFuseTY + 2 * R) * kFuseTX * 3;             // 2R+1
-    const int x0 = blockIdx.x * kFuseTX, y0 = blockIdx.y * kFuseTY;
+__global__ void __launch_bounds__(kVThreads) post_v_kernel(const PostParams pp,
+                                                            const float4* __restrict__ hdr,
+                                                            const float4* __restrict__ bloom,
+                                                            uint32_t* __restrict__ image) {
+    extern __shared__ float smemf[];
+    const int R = pp.active ? pp.radius : 0;
+    float* w = smemf;                 // 2R + 2
+    float* wsum = w + 2 * R + 2;      // kVRows
     const int tid = threadIdx.x;
-    for (int i = tid; i <= 2 * R; i += kFuseThreads) w[i] = tap_weight(i - R, pp.sigma);
-    const int rows = kFuseTY + 2 * R;
-    for (int c0 = 0; c0 < rows; c0 += kFuseChunk) {
+    const int x0 = blockIdx.x * kVCols, y0 = blockIdx.y * kVRows;
+    if (pp.active) {
+        load_weights(w, R, pp.sigma, tid, blockDim.x);
         __syncthreads();
-        const int nrow = min(kFuseChunk, rows - c0);
-        for (int j = tid; j < nrow * segw; j += kFuseThreads) {
-            const int r = j / segw, cx = j - r * segw;
-            const int gy = y0 - R + c0 + r, gx = x0 - R + cx;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (gy >= 0 && gy < pp.height && gx >= 0 && gx < pp.width)
-                v = bloom_source(__ldg(hdr + (size_t)gy * pp.width + gx), pp);
-            stage[j] = v;
-        }
+        if (tid < kVRows) wsum[tid] = weight_sum(y0 + tid, pp.height, w, R);
         __syncthreads();
-        for (int j = tid; j < nrow * kFuseTX; j += kFuseThreads) {
-            const int r = j / kFuseTX, cx = j - r * kFuseTX;
-            const int x = x0 + cx;
-            float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
-            for (int i = -R; i <= R; ++i) {
-                const int sx = x + i;
-                if (sx < 0 || sx >= pp.width) continue;
-                const float wi = w[i + R];
-                const float4 c = stage[r * segw + cx + R + i];
-                ax += c.x * wi;
-                ay += c.y * wi;
-                az += c.z * wi;
-                ws += wi;
-            }
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    const int x = x0 + (warp & 1) * 32 + lane;
+    const int rb = (warp >> 1) * kBJ;
+    const int yb = y0 + rb;
+    if (x >= pp.width || yb >= pp.height) return;
+    float acc[kBJ][3];
+    if (pp.active) {
+        const float4* col = bloom + x;
+        const int W = pp.width;
+        auto load = [col, yb, R, W](int k) { return __ldg(col + (size_t)(yb - R + k) * W); };
+        if (2 * R >= kBJ - 1 && yb - R >= 0 && yb + kBJ - 1 + R < pp.height)
+            blur_interior(load, w, R, acc);
+        else
+            blur_edge(load, w, R, yb, pp.height, acc);
+    }
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j) {
+        const int y = yb + j;
+        if (y >= pp.height) break;
+        const size_t idx = (size_t)y * pp.width + x;
+        const float4 base = __ldg(hdr + idx);
+        float fr = base.x, fg = base.y, fb = base.z;
+        if (pp.active) {
+            const float ws = wsum[rb + j];
+            float ax = acc[j][0], ay = acc[j][1], az = acc[j][2];
             if (ws > 0.0f) {
                 ax /= ws;
                 ay /= ws;
                 az /= ws;
             }
-            float* o = hb + ((c0 + r) * kFuseTX + cx) * 3;
-            o[0] = ax;
-            o[1] = ay;
-            o[2] = az;
+            fr += ax * pp.intensity;
+            fg += ay * pp.intensity;
+            fb += az * pp.intensity;
         }
-    }
-    __syncthreads();
-    for (int j = tid; j < kFuseTX * kFuseTY; j += kFuseThreads) {
-        const int ry = j / kFuseTX, cx = j - ry * kFuseTX;
-        const int x = x0 + cx, y = y0 + ry;
-        if (x >= pp.width || y >= pp.height) continue;
-        const size_t idx = (size_t)y * pp.width + x;
-        const float4 base = __ldg(hdr + idx);
-        float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
-        for (int i = -R; i <= R; ++i) {
-            const int sy = y + i;
-            if (sy < 0 || sy >= pp.height) continue;
-            const float wi = w[i + R];
-            const float* c = hb + ((ry + R + i) * kFuseTX + cx) * 3;
-            ax += c[0] * wi;
-            ay += c[1] * wi;
-            az += c[2] * wi;
-            ws += wi;
-        }
-        if (ws > 0.0f) {
-            ax /= ws;
-            ay /= ws;
-            az /= ws;
-        }
-        image[idx] = tone_pack(base.x + ax * pp.intensity, base.y + ay * pp.intensity,
-                               base.z + az * pp.intensity);
+        image[idx] = tone_pack(fr, fg, fb);
     }
 }
 
@@ -657,12 +697,10 @@ __global__ void tonemap_kernel(const PostParams pp, const float4* __restrict__ h
     }
 }
 
-static size_t bloom_h_smem(int R) { return (size_t)(kRowSeg + 2 * R) * sizeof(float4) + (size_t)(2 * R + 1) * sizeof(float); }
-static size_t post_v_smem(int R) { return (size_t)(kPostTY + 2 * R) * kPostTX * sizeof(float4) + (size_t)(2 * R + 1) * sizeof(float); }
-static size_t post_fused_smem(int R) {
-    return (size_t)kFuseChunk * (kFuseTX + 2 * R) * sizeof(float4) +
-           (size_t)(kFuseTY + 2 * R) * kFuseTX * 3 * sizeof(float) + (size_t)(2 * R + 1) * sizeof(float);
+static size_t bloom_h_smem(int R) {
+    return (size_t)kHRows * bloom_h_stride(R) * sizeof(float4) + (size_t)(2 * R + 2 + kHCols) * sizeof(float);
 }
+static size_t post_v_smem(int R) { return (size_t)(2 * R + 2 + kVRows) * sizeof(float); }
 constexpr size_t kSmemLimit = 200 * 1024;
 
 static cudaError_t set_smem(const void* fn, size_t bytes) {
@@ -676,8 +714,8 @@ cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, flo
     if (sm > kSmemLimit) return cudaErrorInvalidValue;
     cudaError_t e = set_smem((const void*)bloom_h_kernel, sm);
     if (e != cudaSuccess) return e;
-    const dim3 grid((pp.width + kRowSeg - 1) / kRowSeg, pp.height);
-    bloom_h_kernel<<<grid, kRowSeg, sm, st>>>(pp, hdr, bloom);
+    const dim3 grid((pp.width + kHCols - 1) / kHCols, (pp.height + kHRows - 1) / kHRows);
+    bloom_h_kernel<<<grid, kHRows * kHWarps, sm, st>>>(pp, hdr, bloom);
     return cudaGetLastError();
 }
 
@@ -688,12 +726,13 @@ cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const f
     if (sm > kSmemLimit) return cudaErrorInvalidValue;
     cudaError_t e = set_smem((const void*)post_v_kernel, sm);
     if (e != cudaSuccess) return e;
-    const dim3 grid((pp.width + kPostTX - 1) / kPostTX, (pp.height + kPostTY - 1) / kPostTY);
-    post_v_kernel<<<grid, dim3(kPostTX, kPostTY), sm, st>>>(pp, hdr, bloom, image);
+    const dim3 grid((pp.width + kVCols - 1) / kVCols, (pp.height + kVRows - 1) / kVRows);
+    post_v_kernel<<<grid, kVThreads, sm, st>>>(pp, hdr, bloom, image);
     return cudaGetLastError();
 }
 
-cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image, cudaStream_t st) {
+cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image, float4* scratch,
+                              cudaStream_t st) {
     if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
     if (!pp.active) {
         int dev = 0, sms = 148;
@@ -702,13 +741,10 @@ cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t*
         tonemap_kernel<<<sms * 8, 256, 0, st>>>(pp, hdr, image);
         return cudaGetLastError();
     }
-    const size_t sm = post_fused_smem(pp.radius);
-    if (sm > kSmemLimit) return cudaErrorInvalidValue;
-    cudaError_t e = set_smem((const void*)post_fused_kernel, sm);
+    if (!scratch) return cudaErrorInvalidValue;
+    const cudaError_t e = launch_bloom_horizontal(pp, hdr, scratch, st);
     if (e != cudaSuccess) return e;
-    const dim3 grid((pp.width + kFuseTX - 1) / kFuseTX, (pp.height + kFuseTY - 1) / kFuseTY);
-    post_fused_kernel<<<grid, kFuseThreads, sm, st>>>(pp, hdr, image);
-    return cudaGetLastError();
+    return launch_post_process(pp, hdr, scratch, image, st);
 }
 
 }  // namespace ktd
