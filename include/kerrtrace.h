@@ -326,6 +326,60 @@ kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning);
 kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev);
 void kt_renderer_destroy(kt_renderer* r);
 
+/* ---- differentiable trace (discrete adjoint) ------------------------------------------------
+ * No counterpart in the reference (its renderer is forward only).  The image is the linear HDR
+ * of a stated-physics trace (KT_MODE_SPEC, spp 1, disk noise off, FP32 or FP64) seen by an orbit
+ * camera; its parameters theta are the spin, the observer inclination (degrees from the spin
+ * axis), a multiplier of the view's base disk temperature scale and the disk outer radius.
+ *
+ *   kt_diff_forward   renders at theta and records, per ray, every accepted step size and the
+ *                     state every 32 accepted steps (the adjoint's checkpoints);
+ *   kt_diff_backward  vector-Jacobian product: grad_out[0..3] = d(sum_p dl_dhdr[p] . hdr[p]) /
+ *                     d theta for the recorded frozen-step model (step sizes held fixed);
+ *   kt_diff_replay    the recorded step sequence at another theta (the frozen-step model whose
+ *                     central differences the adjoint matches); flags_out[p] = 1 where the
+ *                     ray's events (termination, shaded crossings) differ from the record, so
+ *                     that discontinuous pixels can be masked.
+ * All three are stream-ordered; the records live in the kt_diff object, sized by
+ * segment_capacity (segments of 32 steps; 0 = 4 per pixel).  A ray whose record does not fit
+ * renders normally but carries no gradient; kt_diff_get_info reports how many.  The FP64 path
+ * takes theta, the camera and the disk LUT in double and accumulates colour in double. */
+typedef struct kt_diff kt_diff;
+typedef struct kt_diff_params {
+    double spin;
+    double inclination_deg;
+    double temperature_scale;  /* disk_temperature_scale = view.base_temperature_scale * this */
+    double disk_outer_radius;
+} kt_diff_params;
+typedef struct kt_diff_view {
+    float observer_r;              /* Kerr-Schild radius of the camera */
+    float azimuth_deg;
+    float fov_deg;                 /* vertical field of view */
+    float base_temperature_scale;
+} kt_diff_view;
+typedef struct kt_diff_info {
+    uint64_t segments_used, segments_capacity;
+    uint64_t overflow_rays;  /* rays without a complete record (no gradient) */
+    uint64_t record_bytes;   /* bytes of records written by the last forward */
+    uint64_t device_bytes;   /* device memory the object holds */
+} kt_diff_info;
+
+/* cfg: the fixed scene (resolution, tolerance, LUTs, ...); its spin, disk outer radius and
+ * temperature scale are replaced by theta at each call. */
+kt_status kt_diff_create(const kt_config* cfg, const kt_diff_view* view, uint32_t segment_capacity, int device,
+                         kt_diff** out);
+kt_status kt_diff_forward(kt_diff* d, void* stream, const kt_diff_params* theta, float* hdr_out, uint32_t* err_word);
+/* hdr64_out: optional (NULL), 3 doubles per pixel: the linear colour before the float store. */
+kt_status kt_diff_replay(kt_diff* d, void* stream, const kt_diff_params* theta, float* hdr_out, double* hdr64_out,
+                         uint32_t* flags_out, uint32_t* err_word);
+/* dl_dhdr: device float4 per pixel (w ignored); grad_out: device, 4 doubles (overwritten). */
+kt_status kt_diff_backward(kt_diff* d, void* stream, const float* dl_dhdr, double* grad_out);
+kt_status kt_diff_get_info(kt_diff* d, kt_diff_info* info);  /* synchronises with the device */
+/* The orbit camera of the diff trace and its derivative in the inclination (degrees). */
+kt_status kt_diff_orbit_camera(float observer_r, float inclination_deg, float azimuth_deg, float fov_deg,
+                               kt_camera* cam, kt_camera* dcam_dincl);
+void kt_diff_destroy(kt_diff* d);
+
 #ifdef __cplusplus
 }
 #endif

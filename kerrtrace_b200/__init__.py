@@ -98,6 +98,28 @@ class KtTuning(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class KtDiffParams(C.Structure):
+    """Mirror of ``kt_diff_params``: the differentiable parameters theta."""
+
+    _fields_ = [("spin", C.c_double), ("inclination_deg", C.c_double), ("temperature_scale", C.c_double),
+                ("disk_outer_radius", C.c_double)]
+
+    def as_list(self) -> list[float]:
+        return [self.spin, self.inclination_deg, self.temperature_scale, self.disk_outer_radius]
+
+
+class KtDiffView(C.Structure):
+    """Mirror of ``kt_diff_view``: the fixed part of the differentiable view."""
+
+    _fields_ = [("observer_r", C.c_float), ("azimuth_deg", C.c_float), ("fov_deg", C.c_float),
+                ("base_temperature_scale", C.c_float)]
+
+
+class KtDiffInfo(C.Structure):
+    _fields_ = [("segments_used", C.c_uint64), ("segments_capacity", C.c_uint64), ("overflow_rays", C.c_uint64),
+                ("record_bytes", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
 class KtJob(C.Structure):
     """Mirror of ``kt_job``: one render of a batch."""
 
@@ -144,6 +166,16 @@ SIGNATURES = [
     ("kt_post_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_trace_noalloc", C.c_int, [C.POINTER(KtConfig), C.POINTER(KtCamera), C.c_uint32, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_diff_create", C.c_int, [C.POINTER(KtConfig), C.POINTER(KtDiffView), C.c_uint32, C.c_int,
+                                 C.POINTER(C.c_void_p)]),
+    ("kt_diff_forward", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtDiffParams), C.c_void_p, C.c_void_p]),
+    ("kt_diff_replay", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtDiffParams), C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
+    ("kt_diff_backward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_diff_get_info", C.c_int, [C.c_void_p, C.POINTER(KtDiffInfo)]),
+    ("kt_diff_orbit_camera", C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(KtCamera),
+                                       C.POINTER(KtCamera)]),
+    ("kt_diff_destroy", None, [C.c_void_p]),
     ("kt_batch_create", C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
     ("kt_batch_set_block", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     ("kt_batch_set_camera", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(KtCamera)]),
@@ -315,6 +347,58 @@ class Context:
     def close(self):
         if self.handle:
             lib().kt_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def diff_orbit_camera(observer_r: float, incl_deg: float, azimuth_deg: float, fov_deg: float):
+    """The differentiable trace's orbit camera and its derivative in the inclination (degrees)."""
+    cam, dcam = KtCamera(), KtCamera()
+    check(lib().kt_diff_orbit_camera(observer_r, incl_deg, azimuth_deg, fov_deg, C.byref(cam), C.byref(dcam)))
+    return cam, dcam
+
+
+class Diff:
+    """Differentiable trace (kt_diff_*): forward with step records, frozen-step replay and the
+    discrete adjoint of the linear HDR image in (spin, inclination, temperature scale, r_out)."""
+
+    def __init__(self, cfg: KtConfig, view: KtDiffView, segment_capacity: int = 0, device: int = 0):
+        self.cfg = cfg.copy()
+        self.view = view
+        h = C.c_void_p()
+        check(lib().kt_diff_create(C.byref(self.cfg), C.byref(view), segment_capacity, device, C.byref(h)))
+        self.handle = h
+
+    @staticmethod
+    def params(theta) -> KtDiffParams:
+        return theta if isinstance(theta, KtDiffParams) else KtDiffParams(*[float(v) for v in theta])
+
+    def forward(self, theta, hdr_ptr: int, err_ptr: int, stream: int = 0):
+        p = self.params(theta)
+        check(lib().kt_diff_forward(self.handle, C.c_void_p(stream), C.byref(p), C.c_void_p(hdr_ptr),
+                                    C.c_void_p(err_ptr)))
+
+    def replay(self, theta, hdr_ptr: int, flags_ptr: int, err_ptr: int, stream: int = 0, hdr64_ptr: int = 0):
+        p = self.params(theta)
+        check(lib().kt_diff_replay(self.handle, C.c_void_p(stream), C.byref(p), C.c_void_p(hdr_ptr),
+                                   C.c_void_p(hdr64_ptr or None), C.c_void_p(flags_ptr or None), C.c_void_p(err_ptr)))
+
+    def backward(self, dl_dhdr_ptr: int, grad_ptr: int, stream: int = 0):
+        check(lib().kt_diff_backward(self.handle, C.c_void_p(stream), C.c_void_p(dl_dhdr_ptr), C.c_void_p(grad_ptr)))
+
+    def info(self) -> KtDiffInfo:
+        i = KtDiffInfo()
+        check(lib().kt_diff_get_info(self.handle, C.byref(i)))
+        return i
+
+    def close(self):
+        if self.handle:
+            lib().kt_diff_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -66,11 +66,19 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     log = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-use_fast_math", "-Xptxas", "-v",
                 "-Xcompiler", "-fPIC", *inc, "-c", str(CSRC / "kt_noalloc.cu"), "-o", str(n_obj)])
     (BUILD / "ptxas_kt_noalloc.txt").write_text(log)
+    d_obj = BUILD / "kt_diff.o"
+    log = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-use_fast_math", "-Xptxas", "-v",
+                "-Xcompiler", "-fPIC", *inc, "-c", str(CSRC / "kt_diff.cu"), "-o", str(d_obj)])
+    (BUILD / "ptxas_kt_diff.txt").write_text(log)
     gxx = shutil.which("g++") or "g++"
     _run([gxx, "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", *inc,
           "-I", str(cuda_home / "include"), "-c", str(CSRC / "kt_host.cpp"), "-o", str(h_obj)])
+    dh_obj = BUILD / "kt_diff_host.o"
+    _run([gxx, "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", *inc,
+          "-I", str(cuda_home / "include"), "-c", str(CSRC / "kt_diff_host.cpp"), "-o", str(dh_obj)])
     tmp = LIB.with_suffix(".so.tmp")
-    _run([nvcc, *ARCH, "-shared", "-cudart", "static", str(k_obj), str(n_obj), str(h_obj), "-o", str(tmp)])
+    _run([nvcc, *ARCH, "-shared", "-cudart", "static", str(k_obj), str(n_obj), str(d_obj), str(h_obj), str(dh_obj),
+          "-o", str(tmp)])
     os.replace(tmp, LIB)
     return LIB
 

@@ -289,7 +289,7 @@ __device__ __forceinline__ double asin_r(double x) { return asin(x); }
 __device__ __forceinline__ float fmod_r(float a, float b) { return fmodf(a, b); }
 __device__ __forceinline__ double fmod_r(double a, double b) { return fmod(a, b); }
 template <class R>
-__device__ __forceinline__ float sky_value(R dx, R dy, R dz, float tau, const Scene& sc) {
+__device__ __forceinline__ R sky_value(R dx, R dy, R dz, R tau, const Scene& sc) {
     const R lon = Ops<R>::atan2r(dz, dx);
     const R lat = asin_r(dy);
     const R spacing = (R)sc.sky_spacing;
@@ -299,13 +299,13 @@ __device__ __forceinline__ float sky_value(R dx, R dy, R dz, float tau, const Sc
     const bool on_line = (dlon < thick || dlon > (spacing - thick)) ||
                          (dlat < thick || dlat > (spacing - thick)) ||
                          (Ops<R>::absr(lat) < thick * R(3));
-    return on_line ? (float)(sc.sky_intensity * (double)tau) : 0.0f;
+    return on_line ? (R)(sc.sky_intensity * (double)tau) : R(0);
 }
 
 // ---- LUT sampling ------------------------------------------------------------------------
 // Software form of a 1D linear, normalised, clamped texture fetch (full-precision weight).
-template <class R>
-__device__ __forceinline__ R lut_lerp1(const float* __restrict__ lut, int n, R u) {
+template <class R, class E = float>
+__device__ __forceinline__ R lut_lerp1(const E* __restrict__ lut, int n, R u) {
     const R x = u * R(n) - R(0.5);
     const R fl = floor(x);
     const R w = x - fl;

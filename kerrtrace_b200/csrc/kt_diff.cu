@@ -1,0 +1,713 @@
+// kt_diff.cu — differentiable trace (stated physics, spp 1, no disk noise).
+//
+// Three kernels share the ray code of the renderer (ray_advance<R, 1, true>), so the recorded
+// forward image is bit for bit the stated-physics trace of the same scene (float path):
+//
+//   diff_forward_kernel<R, false>  adaptive trace; appends each accepted step size to the ray's
+//                                  segment records (state + transmittance at every kSegSteps-th
+//                                  step), writes the ray's event summary.
+//   diff_forward_kernel<R, true>   frozen-step replay: the recorded step sizes, one attempt each
+//                                  (max_attempts = 1 in the scene), at new parameters; flags the
+//                                  rays whose events differ from the record.  Central
+//                                  differences of the frozen-step model use it.
+//   diff_backward_kernel<R>        discrete adjoint.  Per ray, from the last segment back: replay
+//                                  the segment forward (states before each step, crossings), then
+//                                  reverse each step:
+//     * crossing: the hit is the dense-output point at the root t* of y(t) = 0; its shading
+//       (disk test, redshift, LUT temperature, blackbody, alpha) is differentiated with duals
+//       in the hit state, p_t, k_t, spin, temperature scale and r_out; the transmittance chain
+//       col += c a tau, tau' = tau (1 - a) is reversed; t* is differentiated by the
+//       implicit-function theorem (dt* = -dy / y'(t*)) and the dense output's linear weights
+//       carry the adjoint to the step's end points and stages;
+//     * step: reverse of the explicit Runge-Kutta map with the step size frozen.  The
+//       vector-Jacobian product of the right-hand side uses that f = J grad H is Hamiltonian:
+//       J_f^T l = J^T J_f (J^T l), a forward (dual-number) JVP of hamilton_rhs in direction
+//       J^T l = (-l_p, l_x); the same dual evaluation gives l . df/d(spin) and l . df/d(p_t).
+//   At the start, the null initialisation is differentiated with duals in spin and
+//   inclination (the camera's inclination tangent comes from the host).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kt_diff.h"
+#include "kt_dual.cuh"
+#include "kt_internal.h"
+#include "kt_ray.cuh"
+
+namespace ktd {
+
+namespace {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+template <class R>
+__device__ __forceinline__ DiffSeg<R>* seg_at(const DiffRecRaw& rec, int i) {
+    return reinterpret_cast<DiffSeg<R>*>(rec.segs) + i;
+}
+
+// Kind of ending of a ray whose advance() just returned true (same tests, same order as
+// ray_advance): NaN state, inside the horizon, beyond the escape radius, else the budget.
+template <class R>
+__device__ __forceinline__ int classify_end(const RayRun<R>& ry, const Scene& sc) {
+    if (Ops<R>::isnanr(ry.s[1])) return kTermFrozen;
+    const R r_now = ks_radius<R>(ry.s[0], ry.s[1], ry.s[2], sc_aa<R>(sc));
+    if (inside_horizon<R>(r_now, sc)) return kTermHorizon;
+    if (beyond_escape<R>(r_now, sc)) return kTermEscape;
+    return kTermBudget;
+}
+
+// Sky value at transmittance 1 in the escape direction of state s (ray_advance's escape branch).
+template <class R>
+__device__ __forceinline__ R escape_sky(const R* s, R pt, const Scene& sc) {
+    using O = Ops<R>;
+    R ke[6];
+    hamilton_rhs<R, true>(s, pt, sc_a<R>(sc), sc_aa<R>(sc), sc_M<R>(sc), ke);
+    const R inv = O::rsq(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
+    return sky_value<R>(ke[0] * inv, ke[1] * inv, ke[2] * inv, R(1), sc);
+}
+
+}  // namespace
+
+// ---- adjoint helpers ---------------------------------------------------------------------------
+
+// Weights of the dense output in (y0, y1, k1, k3, k4, k5, k6, k7): it is linear in them.
+template <class R>
+__device__ __forceinline__ void dense_weights(R t, R h, R w[8]) {
+    using C = DP<R>;
+    const R t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+    const R q2 = t, q3 = t - t2, q4 = t2 - t3, q5 = t2 - R(2) * t3 + t4;
+    w[0] = R(1) - q2 + q3 - R(2) * q4;
+    w[1] = q2 - q3 + R(2) * q4;
+    w[2] = h * (q3 - q4 + C::d1 * q5);
+    w[3] = h * (C::d3 * q5);
+    w[4] = h * (C::d4 * q5);
+    w[5] = h * (C::d5 * q5);
+    w[6] = h * (C::d6 * q5);
+    w[7] = h * (-q4 + C::d7 * q5);
+}
+
+// l^T df/dY at Y (out), l . df/d(spin) (da) and l . df/d(p_t) (dpt), from one dual evaluation
+// of the right-hand side in direction (J^T l, d spin, d p_t).
+template <class R>
+__device__ __forceinline__ void rhs_vjp(const R* Y, const R* l, R pt, R a, R aa, R M, R* out, R& da, R& dpt) {
+    using D = Dual<R, 3>;
+    D st[6], d[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) st[c] = D(Y[c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        st[c].d[0] = -l[c + 3];
+        st[c + 3].d[0] = l[c];
+    }
+    D Da(a), Daa(aa), Dpt(pt), DM(M);
+    Da.d[1] = R(1);
+    Daa.d[1] = R(2) * a;
+    Dpt.d[2] = R(1);
+    hamilton_rhs<D, true>(st, Dpt, Da, Daa, DM, d);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        out[c] = -d[c + 3].d[0];
+        out[c + 3] = d[c].d[0];
+    }
+    R sa = R(0), sp = R(0);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        sa += l[c] * d[c].d[1];
+        sp += l[c] * d[c].d[2];
+    }
+    da = sa;
+    dpt = sp;
+}
+
+// Tangent slots of the shading duals.
+enum : int { kSX = 0, kSPt = 6, kSKt = 7, kSA = 8, kSTs = 9, kSRo = 10, kSN = 11 };
+
+// Disk shading of hit state X (shade_hit<R, 1> without noise) on duals: returns false where the
+// hit is not shaded; else the blackbody colour c and the opacity alpha with their derivatives.
+template <class R>
+__device__ bool shade_dual(const R* X, R pt, R kt, const Scene& sc, const DiffLut& dl, Dual<R, kSN>* c3,
+                           Dual<R, kSN>& alpha) {
+    using D = Dual<R, kSN>;
+    using O = Ops<D>;
+    D h[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) h[c] = D::seed(X[c], kSX + c);
+    const D Dpt = D::seed(pt, kSPt), Dkt = D::seed(kt, kSKt);
+    const D a = D::seed(sc_a<R>(sc), kSA);
+    const D aa = a * a;
+    const R M = sc_M<R>(sc);
+    D r_in(sizeof(R) == 8 ? (R)sc.disk_inner_d : (R)sc.disk_inner);
+    r_in.d[kSA] = (R)dl.dr_in_da;
+    const D r_out = D::seed(sizeof(R) == 8 ? (R)sc.disk_outer_d : (R)sc.disk_outer, kSRo);
+    const D xh = h[0], zh = h[2], pxh = h[3], pzh = h[5];
+    const D rh = ks_radius<D>(xh, D(R(0)), zh, aa);
+    if (!(rh >= r_in && rh <= r_out)) return false;
+    const R sqM = Ops<R>::sqrt_rn(M);
+    const D rs = O::sqrt_rn(rh);
+    const D disc = R(1) - R(3) * M / rh + R(2) * sqM * a / (rh * rs);
+    if (!(disc.v > R(0))) return false;
+    const D omega = -sqM / (rh * rs + a * sqM);
+    const D r2h = rh * rh;
+    const D inv = R(1) / (r2h + aa);
+    const D lx = (rh * xh - a * zh) * inv;
+    const D lz = (rh * zh + a * xh) * inv;
+    const D ldotp = O::fma(lx, pxh, lz * pzh);
+    const D ldotxi = lx * zh - lz * xh;
+    const D Hk = M * rh * r2h / (r2h * r2h);
+    const D L = (zh * pxh - xh * pzh) + R(2) * Hk * ldotxi * (ldotp + Dkt);
+    const D energy = -Dpt;
+    const D l_over_e = L / energy;
+    const D g = R(1) / (O::rsq(disc) * (R(1) - omega * l_over_e));
+    const D span = r_out - r_in;
+    const D u = span.v > R(0) ? (rh - r_in) / span : D(R(0));
+    // disk LUT, software linear fetch (lut_lerp1); the entries carry their spin / r_out tangents
+    const int n = sc.lut_size;
+    const D x = u * R(n) - R(0.5);
+    const R fl = floor(x.v);
+    const R flc = fl < R(-1) ? R(-1) : (fl > R(n - 1) ? R(n - 1) : fl);
+    int i0 = fl == fl ? (int)flc : 0;
+    int i1 = i0 + 1;
+    i0 = i0 < 0 ? 0 : i0;
+    i1 = i1 > n - 1 ? n - 1 : i1;
+    const bool lut_d = sizeof(R) == 8 && sc.disk_lut_d;
+    D v0(lut_d ? (R)__ldg(sc.disk_lut_d + i0) : (R)__ldg(sc.disk_lut + i0));
+    D v1(lut_d ? (R)__ldg(sc.disk_lut_d + i1) : (R)__ldg(sc.disk_lut + i1));
+    v0.d[kSA] = (R)__ldg(dl.dlut_da + i0);
+    v1.d[kSA] = (R)__ldg(dl.dlut_da + i1);
+    v0.d[kSRo] = (R)__ldg(dl.dlut_dro + i0);
+    v1.d[kSRo] = (R)__ldg(dl.dlut_dro + i1);
+    const D w = x - fl;
+    const D sampled = v0 + w * (v1 - v0);
+    D ts((R)sc.temp_scale);
+    ts.d[kSTs] = (R)dl.dtemp_ds;
+    const D T = ts * sampled * g;
+    if (!(Ops<R>::isfiniter(T.v) && T.v > R(0))) return false;
+    // blackbody LUT (blackbody_rgb<1> / blackbody_rgb_d): linear in T between two entries
+    if (T.v > (R)sc.lut_max_temp) {
+        c3[0] = c3[1] = c3[2] = D(R(0));
+        alpha = D(R(0));
+        return true;
+    }
+    const int nb = sc.lut_size;
+    const D pos = T / (R)sc.lut_max_temp * R(nb - 1);
+    const R fb = floor(pos.v);
+    const R fbc = fb < R(-1) ? R(-1) : (fb > R(nb - 1) ? R(nb - 1) : fb);
+    int j0 = fb == fb ? (int)fbc : 0;
+    int j1 = j0 + 1;
+    j0 = j0 < 0 ? 0 : j0;
+    j1 = j1 > nb - 1 ? nb - 1 : j1;
+    const float4 ca = __ldg(sc.bb_lut + j0), cb = __ldg(sc.bb_lut + j1);
+    const D wb = pos - fb;
+    c3[0] = (R)ca.x + wb * (R)(cb.x - ca.x);
+    c3[1] = (R)ca.y + wb * (R)(cb.y - ca.y);
+    c3[2] = (R)ca.z + wb * (R)(cb.z - ca.z);
+    const D luma = R(0.2126) * c3[0] + R(0.7152) * c3[1] + R(0.0722) * c3[2];
+    const D luma_s = luma / (R)sc.wl_step;
+    alpha = R(1) - O::expr(luma_s * R(-0.5));
+    return true;
+}
+
+// Null initialisation of ray_start on any number type (values, or duals for its derivatives):
+// p_t from the null condition with the "-sqrt" root, p = n + 2 Hk l (k_t + l.n).
+template <class T, class R>
+__device__ __forceinline__ void start_state(const T* pos, const T* dirv, T a, R M, T* s, T& pt, T& kt) {
+    using O = Ops<T>;
+    const T aa = a * a;
+    const T inv_n = O::rsq(dirv[0] * dirv[0] + dirv[1] * dirv[1] + dirv[2] * dirv[2]);
+    const T nx = dirv[0] * inv_n, ny = dirv[1] * inv_n, nz = dirv[2] * inv_n;
+    const T x = pos[0], y = pos[1], z = pos[2];
+    const T rho2 = O::fma(x, x, O::fma(y, y, z * z));
+    const T uu = rho2 - aa;
+    const T s_term = O::sqrt_rn(O::fma(uu, uu, R(4) * aa * y * y));
+    const T r2 = R(0.5) * (uu + s_term);
+    const T r = O::sqrt_rn(r2);
+    const T den = r2 + aa;
+    const T inv_den = O::fdiv(T(R(1)), den);
+    const T lx = (r * x - a * z) * inv_den;
+    const T ly = O::fdiv(y, r);
+    const T lz = (r * z + a * x) * inv_den;
+    const T denH = O::fma(r2, r2, aa * y * y);
+    const T Hk = M * r2 * r * O::fdiv(T(R(1)), denH);
+    const T ln = O::fma(lx, nx, O::fma(ly, ny, lz * nz));
+    const T g_tt = R(-1) + R(2) * Hk;
+    const T g_tn = R(2) * Hk * ln;
+    const T g_nn = R(1) + R(2) * Hk * ln * ln;
+    const T disc = g_tn * g_tn - g_tt * g_nn;
+    kt = (-g_tn - O::sqrt_rn(disc)) / g_tt;
+    pt = g_tt * kt + g_tn;
+    const T w = kt + ln;
+    s[0] = x;
+    s[1] = y;
+    s[2] = z;
+    s[3] = nx + R(2) * Hk * lx * w;
+    s[4] = ny + R(2) * Hk * ly * w;
+    s[5] = nz + R(2) * Hk * lz * w;
+}
+
+// Screen coordinates of a pixel centre (pixel_ray<1> at spp 1), in double.
+__device__ __forceinline__ void pixel_uv(int px, int py, const Scene& sc, double fov, double& u, double& v) {
+    const double W = (double)sc.width, H = (double)sc.height;
+    u = ((px + 0.5) * (2.0 / W) - 1.0) * (W / H) * fov;
+    v = (1.0 - (py + 0.5) * (2.0 / H)) * fov;
+}
+
+// Start of a pixel's ray.  Float: the renderer's start from the float camera (so the record is
+// the renderer's image).  Double: the same initialisation from the double camera.
+template <class R>
+__device__ __forceinline__ bool ray_begin(int px, int py, const Scene& sc, const Camera& cam, const CameraD& camd,
+                                          RayRun<R>& ry) {
+    if constexpr (sizeof(R) == 4) {
+        float dir[3];
+        pixel_ray<1>(px, py, 0, sc, cam, dir);
+        return start(ry, cam, dir, sc);
+    } else {
+        double u, v, dirv[3];
+        pixel_uv(px, py, sc, camd.fov_scale, u, v);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dirv[c] = u * camd.rgt[c] + v * camd.up[c] + camd.fwd[c];
+        start_state<double, double>(camd.pos, dirv, sc.a_d, sc.M_d, ry.s, ry.pt, ry.kt);
+        ry.h = sc.h0_d;
+        ry.tol = 0.0;
+        ry.col[0] = ry.col[1] = ry.col[2] = 0.0;
+        ry.tau = 1.0;
+        ry.step = 0;
+        ry.attempt = 0;
+        ry.have_k1 = false;
+        return 0 < sc.max_steps && 1.0f > sc.cutoff_gt;
+    }
+}
+
+// Start state with derivatives in spin (slot 0) and inclination (slot 1).
+template <class R>
+__device__ __forceinline__ void start_dual(int px, int py, const Scene& sc, const Camera& cam, const CameraD& camd,
+                                           const CameraD& dcamd, Dual<R, 2>* s, Dual<R, 2>& pt, Dual<R, 2>& kt) {
+    using D = Dual<R, 2>;
+    D dirv[3], pos[3];
+    if constexpr (sizeof(R) == 4) {
+        const float u = ((px + 0.5f) * sc.inv_w_2 - 1.0f) * sc.aspect * cam.fov_scale;
+        const float v = (1.0f - (py + 0.5f) * sc.inv_h_2) * cam.fov_scale;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            dirv[c] = D((R)(u * cam.rgt[c] + v * cam.up[c] + cam.fwd[c]));
+            dirv[c].d[1] = (R)(u * dcamd.rgt[c] + v * dcamd.up[c] + dcamd.fwd[c]);
+            pos[c] = D((R)cam.pos[c]);
+            pos[c].d[1] = (R)dcamd.pos[c];
+        }
+    } else {
+        double u, v;
+        pixel_uv(px, py, sc, camd.fov_scale, u, v);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            dirv[c] = D(u * camd.rgt[c] + v * camd.up[c] + camd.fwd[c]);
+            dirv[c].d[1] = u * dcamd.rgt[c] + v * dcamd.up[c] + dcamd.fwd[c];
+            pos[c] = D(camd.pos[c]);
+            pos[c].d[1] = dcamd.pos[c];
+        }
+    }
+    start_state<D, R>(pos, dirv, D::seed(sc_a<R>(sc), 0), sc_M<R>(sc), s, pt, kt);
+}
+
+// Stages of one DP5 step from s with step h (ray_advance's expressions): k[0..6] = k1..k7,
+// nx = the 5th-order state.
+template <class R>
+__device__ __forceinline__ void dp5_stages(const R* s, R h, R pt, R a, R aa, R M, R (*k)[6], R* nx) {
+    using C = DP<R>;
+    R y[6];
+    hamilton_rhs<R, true>(s, pt, a, aa, M, k[0]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * C::a21 * k[0][c];
+    hamilton_rhs<R, true>(y, pt, a, aa, M, k[1]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a31 * k[0][c] + C::a32 * k[1][c]);
+    hamilton_rhs<R, true>(y, pt, a, aa, M, k[2]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) y[c] = s[c] + h * (C::a41 * k[0][c] + C::a42 * k[1][c] + C::a43 * k[2][c]);
+    hamilton_rhs<R, true>(y, pt, a, aa, M, k[3]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        y[c] = s[c] + h * (C::a51 * k[0][c] + C::a52 * k[1][c] + C::a53 * k[2][c] + C::a54 * k[3][c]);
+    hamilton_rhs<R, true>(y, pt, a, aa, M, k[4]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        y[c] = s[c] + h * (C::a61 * k[0][c] + C::a62 * k[1][c] + C::a63 * k[2][c] + C::a64 * k[3][c] +
+                           C::a65 * k[4][c]);
+    hamilton_rhs<R, true>(y, pt, a, aa, M, k[5]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        nx[c] = s[c] + h * (C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] +
+                            C::b6 * k[5][c]);
+    hamilton_rhs<R, true>(nx, pt, a, aa, M, k[6]);
+}
+
+// Runge-Kutta matrix with row 7 = b (the stage-7 input is the 5th-order state).
+template <class R>
+__device__ __forceinline__ R rk_a(int m, int j) {
+    using C = DP<R>;
+    switch (m * 8 + j) {
+        case 2 * 8 + 1: return C::a21;
+        case 3 * 8 + 1: return C::a31;
+        case 3 * 8 + 2: return C::a32;
+        case 4 * 8 + 1: return C::a41;
+        case 4 * 8 + 2: return C::a42;
+        case 4 * 8 + 3: return C::a43;
+        case 5 * 8 + 1: return C::a51;
+        case 5 * 8 + 2: return C::a52;
+        case 5 * 8 + 3: return C::a53;
+        case 5 * 8 + 4: return C::a54;
+        case 6 * 8 + 1: return C::a61;
+        case 6 * 8 + 2: return C::a62;
+        case 6 * 8 + 3: return C::a63;
+        case 6 * 8 + 4: return C::a64;
+        case 6 * 8 + 5: return C::a65;
+        case 7 * 8 + 1: return C::b1;
+        case 7 * 8 + 3: return C::b3;
+        case 7 * 8 + 4: return C::b4;
+        case 7 * 8 + 5: return C::b5;
+        case 7 * 8 + 6: return C::b6;
+        default: return R(0);
+    }
+}
+
+// ---- forward: record / replay ----------------------------------------------------------------
+template <class R, bool REPLAY>
+__global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const Camera cam, const CameraD camd,
+                                                          const DiffRecRaw rec, float4* __restrict__ hdr,
+                                                          double* __restrict__ hdr64, uint32_t* __restrict__ err,
+                                                          uint32_t* __restrict__ flags) {
+    const unsigned n_px = (unsigned)sc.width * (unsigned)sc.height;
+    const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_px) return;
+    const int px = (int)(p % (unsigned)sc.width), py = (int)(p / (unsigned)sc.width);
+    RayRun<R> ry;
+    Tally tl;
+    tl.clear();
+    const bool started = ray_begin<R>(px, py, sc, cam, camd, ry);
+    if (!REPLAY) {
+        DiffRay out;
+        out.first_seg = out.last_seg = -1;
+        out.n_steps = 0;
+        out.n_hits = 0;
+        out.term = kTermNotStarted;
+        out.sky = 0.0f;
+        if (started) {
+            int cur = -1, in_seg = 0;
+            bool rec_ok = true;
+            DiffSeg<R>* sg = nullptr;
+            while (true) {
+                if (ry.attempt == 0 && in_seg == 0 && rec_ok) {  // a step starts a new segment
+                    const unsigned idx = atomicAdd(rec.seg_count, 1u);
+                    if (idx >= rec.cap) {
+                        rec_ok = false;
+                        atomicAdd(rec.status, 1u);
+                    } else {
+                        sg = seg_at<R>(rec, (int)idx);
+                        sg->prev = cur;
+                        sg->next = -1;
+                        sg->n = 0;
+                        sg->first_step = out.n_steps;
+                        sg->tau = ry.tau;
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) sg->s[c] = ry.s[c];
+                        if (cur >= 0) seg_at<R>(rec, cur)->next = (int)idx;
+                        else out.first_seg = (int)idx;
+                        cur = (int)idx;
+                    }
+                }
+                const R h_used = ry.h;
+                const bool done = advance<1, true>(ry, sc, err, tl);
+                if (ry.attempt != 0) continue;  // rejected attempt: the step is retried
+                if (Ops<R>::isnanr(ry.s[1])) {  // frozen: this step is not part of the record
+                    out.term = kTermFrozen;
+                    break;
+                }
+                if (rec_ok) {
+                    sg->h[in_seg] = h_used;
+                    sg->n = ++in_seg;
+                    out.last_seg = cur;
+                    if (in_seg == kSegSteps) in_seg = 0;
+                }
+                ++out.n_steps;
+                if (done) {
+                    out.term = classify_end<R>(ry, sc);
+                    if (out.term == kTermEscape) out.sky = (float)escape_sky<R>(ry.s, ry.pt, sc);
+                    break;
+                }
+            }
+            if (!rec_ok) out.term = kTermOverflow;
+            // a segment opened by a step that froze holds no step: drop it from the list
+            if (rec_ok && sg && sg->n == 0) {
+                out.last_seg = sg->prev;
+                if (sg->prev >= 0) seg_at<R>(rec, sg->prev)->next = -1;
+                else out.first_seg = -1;
+            }
+        }
+        out.n_hits = (int)tl.hits;
+        rec.rays[p] = out;
+    } else {
+        const DiffRay rr = rec.rays[p];
+        uint32_t flip = 0;
+        int n_done = 0;
+        int term = kTermNotStarted;
+        if (started != (rr.term != kTermNotStarted)) flip = 1;
+        if (started && rr.term != kTermNotStarted && rr.term != kTermOverflow) {
+            bool done = false;
+            for (int si = rr.first_seg; si >= 0 && !done; si = seg_at<R>(rec, si)->next) {
+                const DiffSeg<R>* sg = seg_at<R>(rec, si);
+                for (int j = 0; j < sg->n && !done; ++j) {
+                    ry.h = sg->h[j];
+                    done = advance<1, true>(ry, sc, err, tl);  // one attempt: always a commit
+                    ++n_done;
+                }
+            }
+            // a recorded ray that froze stops after its last recorded step (the NaN step adds
+            // nothing to the image)
+            if (done) term = classify_end<R>(ry, sc);
+            else term = rr.term == kTermFrozen ? kTermFrozen : -1;
+            if (term != rr.term || n_done != rr.n_steps || (int)tl.hits != rr.n_hits) flip = 1;
+        } else if (rr.term == kTermOverflow) {
+            flip = 1;
+        }
+        if (flags) flags[p] = flip;
+    }
+    const float fs = sc.final_scale;
+    hdr[p] = make_float4((float)ry.col[0] * fs, (float)ry.col[1] * fs, (float)ry.col[2] * fs, 1.0f);
+    if (hdr64) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) hdr64[3 * (size_t)p + c] = (double)ry.col[c] * (double)fs;
+    }
+}
+
+// ---- adjoint kernel ----------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, const Camera cam, const CameraD camd,
+                                                           const CameraD dcamd, const DiffRecRaw rec, const DiffLut dl,
+                                                           const float4* __restrict__ dl_dhdr,
+                                                           double* __restrict__ grad, uint32_t* __restrict__ err) {
+    const unsigned n_px = (unsigned)sc.width * (unsigned)sc.height;
+    const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    double g[4] = {0.0, 0.0, 0.0, 0.0};
+    if (p < n_px) {
+        const DiffRay rr = rec.rays[p];
+        const float4 dlp = dl_dhdr[p];
+        const R fs = (R)sc.final_scale;
+        const R lc[3] = {(R)dlp.x * fs, (R)dlp.y * fs, (R)dlp.z * fs};
+        // only shaded crossings carry derivatives (the sky grid is piecewise constant)
+        const bool live = rr.term != kTermNotStarted && rr.term != kTermOverflow && rr.last_seg >= 0 &&
+                          rr.n_hits > 0 && (lc[0] != R(0) || lc[1] != R(0) || lc[2] != R(0));
+        if (live) {
+            const int px = (int)(p % (unsigned)sc.width), py = (int)(p / (unsigned)sc.width);
+            RayRun<R> ry0;
+            ray_begin<R>(px, py, sc, cam, camd, ry0);
+            const R pt = ry0.pt, kt = ry0.kt;
+            const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
+            R ls[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};  // adjoint of the current state
+            R lpt = R(0), lkt = R(0), ga = R(0), gts = R(0), gro = R(0);
+            R ltau = rr.term == kTermEscape ? (lc[0] + lc[1] + lc[2]) * (R)rr.sky : R(0);
+            R sj[kSegSteps][6];
+            R tauj[kSegSteps];
+            bool hitj[kSegSteps];
+            for (int si = rr.last_seg; si >= 0;) {
+                const DiffSeg<R>* sg = seg_at<R>(rec, si);
+                const int n = sg->n;
+                // replay the segment: states before each step and its shaded crossings
+                RayRun<R> ry;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) ry.s[c] = sg->s[c];
+                ry.pt = pt;
+                ry.kt = kt;
+                ry.tol = R(0);
+                ry.col[0] = ry.col[1] = ry.col[2] = R(0);
+                ry.tau = sg->tau;
+                ry.step = sg->first_step;
+                ry.attempt = 0;
+                ry.have_k1 = false;
+                Tally tl;
+                tl.clear();
+                for (int j = 0; j < n; ++j) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) sj[j][c] = ry.s[c];
+                    tauj[j] = ry.tau;
+                    const uint32_t hits0 = tl.hits;
+                    ry.h = sg->h[j];
+                    advance<1, true>(ry, sc, err, tl);
+                    hitj[j] = tl.hits != hits0;
+                }
+                // reverse the segment's steps
+                for (int j = n - 1; j >= 0; --j) {
+                    const R h = sg->h[j];
+                    R k[7][6], nx[6];
+                    dp5_stages<R>(sj[j], h, pt, a, aa, M, k, nx);
+                    R ly0[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+                    R ly1[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+                    R dk[7][6];  // adjoints of k1..k7 from the dense output (k2 stays 0)
+#pragma unroll
+                    for (int i = 0; i < 7; ++i)
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) dk[i][c] = R(0);
+                    if (hitj[j]) {
+                        // hit point: the crossing root of shade_crossing<R, 1>
+                        const R* s0 = sj[j];
+                        const R yv0 = s0[1], yv1 = nx[1];
+                        const R dy = yv0 - yv1;
+                        R t = dy != R(0) ? Ops<R>::fdiv(yv0, dy) : R(0.5);
+                        t = Ops<R>::minr(Ops<R>::maxr(t, R(0)), R(1));
+                        t = crossing_root<R>(yv0, yv1, k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], h, t);
+                        R X[6], dX[6];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) {
+                            X[c] = dense_eval<R>(s0[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c],
+                                                 h, t);
+                            dX[c] = dense_slope<R>(s0[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c],
+                                                   k[6][c], h, t);
+                        }
+                        Dual<R, kSN> cc[3], al;
+                        if (shade_dual<R>(X, pt, kt, sc, dl, cc, al)) {
+                            const R tin = tauj[j];
+                            // col += c alpha tau_in ; tau_out = tau_in (1 - alpha)
+                            R q[kSN];
+#pragma unroll
+                            for (int i = 0; i < kSN; ++i) {
+                                R v = R(0);
+#pragma unroll
+                                for (int ch = 0; ch < 3; ++ch) v += lc[ch] * (cc[ch].d[i] * al.v + cc[ch].v * al.d[i]);
+                                q[i] = v * tin - ltau * tin * al.d[i];
+                            }
+                            ltau = (lc[0] * cc[0].v + lc[1] * cc[1].v + lc[2] * cc[2].v) * al.v +
+                                   ltau * (R(1) - al.v);
+                            lpt += q[kSPt];
+                            lkt += q[kSKt];
+                            ga += q[kSA];
+                            gts += q[kSTs];
+                            gro += q[kSRo];
+                            // root: y(t*) = 0  =>  dt* = -(dD_1/din . din) / D_1'(t*)
+                            R lt = R(0);
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) lt += q[kSX + c] * dX[c];
+                            const R mu = dX[1] != R(0) ? -lt / dX[1] : R(0);
+                            R wd[8];
+                            dense_weights<R>(t, h, wd);
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) {
+                                const R e = q[kSX + c] + (c == 1 ? mu : R(0));
+                                ly0[c] += e * wd[0];
+                                ly1[c] += e * wd[1];
+                                dk[0][c] += e * wd[2];
+                                dk[2][c] += e * wd[3];
+                                dk[3][c] += e * wd[4];
+                                dk[4][c] += e * wd[5];
+                                dk[5][c] += e * wd[6];
+                                dk[6][c] += e * wd[7];
+                            }
+                        }
+                    }
+                    // reverse of s' = s + h sum b_i k_i, k_i = f(Y_i), Y_i = s + h sum_j a_ij k_j
+                    R lnext[6], lnew[6];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        lnext[c] = ls[c] + ly1[c];
+                        lnew[c] = lnext[c] + ly0[c];
+                    }
+                    R acc[7][6];  // adjoint of k_i collected so far (i = 0..6 for k1..k7)
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) {
+                        const R b = i < 6 ? rk_a<R>(7, i + 1) : R(0);
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) acc[i][c] = h * b * lnext[c] + dk[i][c];
+                    }
+#pragma unroll
+                    for (int m = 6; m >= 0; --m) {  // stage m + 1
+                        R Y[6];
+                        if (m == 6) {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) Y[c] = nx[c];
+                        } else if (m == 0) {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) Y[c] = sj[j][c];
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) {
+                                R sum = R(0);
+#pragma unroll
+                                for (int jj = 0; jj < m; ++jj) sum += rk_a<R>(m + 1, jj + 1) * k[jj][c];
+                                Y[c] = sj[j][c] + h * sum;
+                            }
+                        }
+                        bool nz = false;
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) nz = nz || acc[m][c] != R(0);
+                        if (!nz) continue;
+                        R lY[6], da, dpt;
+                        rhs_vjp<R>(Y, acc[m], pt, a, aa, M, lY, da, dpt);
+                        ga += da;
+                        lpt += dpt;
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) lnew[c] += lY[c];
+#pragma unroll
+                        for (int i = 0; i < m; ++i) {
+                            const R coef = h * rk_a<R>(m + 1, i + 1);
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) acc[i][c] += coef * lY[c];
+                        }
+                    }
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) ls[c] = lnew[c];
+                }
+                si = sg->prev;
+            }
+            // initial state: s0, p_t, k_t as functions of spin and inclination
+            Dual<R, 2> s0[6], dpt0, dkt0;
+            start_dual<R>(px, py, sc, cam, camd, dcamd, s0, dpt0, dkt0);
+            R gi = R(0);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                ga += ls[c] * s0[c].d[0];
+                gi += ls[c] * s0[c].d[1];
+            }
+            ga += lpt * dpt0.d[0] + lkt * dkt0.d[0];
+            gi += lpt * dpt0.d[1] + lkt * dkt0.d[1];
+            g[0] = (double)ga;
+            g[1] = (double)gi;
+            g[2] = (double)gts;
+            g[3] = (double)gro;
+        }
+    }
+    // warp sums, one atomic per warp and parameter
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        double v = g[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFullMask, v, o);
+        if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(grad + i, v);
+    }
+}
+
+// ---- launchers ----------------------------------------------------------------------------------
+cudaError_t launch_diff_forward(const Scene& sc, const Camera& cam, const CameraD& camd, const DiffRecRaw& rec,
+                                int replay, float4* hdr, double* hdr64, uint32_t* err, uint32_t* flags,
+                                cudaStream_t st) {
+    const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
+    if (n == 0) return cudaSuccess;
+    const dim3 grid((n + 127) / 128);
+    if (sc.precision == 2) {
+        if (replay) diff_forward_kernel<double, true><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
+        else diff_forward_kernel<double, false><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
+    } else {
+        if (replay) diff_forward_kernel<float, true><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
+        else diff_forward_kernel<float, false><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diff_backward(const Scene& sc, const Camera& cam, const CameraD& camd, const CameraD& dcamd,
+                                 const DiffRecRaw& rec, const DiffLut& dl, const float4* dl_dhdr, double* grad,
+                                 uint32_t* err, cudaStream_t st) {
+    const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
+    if (n == 0) return cudaSuccess;
+    const dim3 grid((n + 127) / 128);
+    if (sc.precision == 2)
+        diff_backward_kernel<double><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, err);
+    else
+        diff_backward_kernel<float><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, err);
+    return cudaGetLastError();
+}
+
+}  // namespace ktd

@@ -494,6 +494,9 @@ kt_status fill_scene(kt_context* c) {
     s.a = p.a; s.M = p.m; s.aa = p.aa; s.inv_M = p.inv_m; s.a_norm = p.a_norm; s.rh = p.rh;
     s.disk_inner = p.disk_inner;
     s.disk_outer = cfg.disk_outer_radius;
+    s.disk_inner_d = (double)s.disk_inner;
+    s.disk_outer_d = (double)s.disk_outer;
+    s.disk_lut_d = nullptr;
     s.inv_w_2 = p.inv_w_2; s.inv_h_2 = p.inv_h_2; s.aspect = p.aspect_ratio;
     s.noise_scale = p.disk_noise_scale; s.noise_strength = p.disk_noise_strength;
     s.noise_winding = p.disk_noise_winding; s.noise_enabled = p.disk_noise_enabled;

@@ -42,14 +42,18 @@ template <> __device__ __forceinline__ double sc_h0<double>(const Scene& s) { re
 template <> __device__ __forceinline__ double sc_tol<double>(const Scene& s) { return s.base_tol_d; }
 template <> __device__ __forceinline__ bool inside_horizon<double>(double r, const Scene& s) { return r < s.horizon_d; }
 template <> __device__ __forceinline__ bool beyond_escape<double>(double r, const Scene& s) { return r > s.escape_d; }
+// transmittance above the cutoff (float: the exact float form of the reference's compare)
+template <class R> __device__ __forceinline__ bool tau_alive(R tau, const Scene& s);
+template <> __device__ __forceinline__ bool tau_alive<float>(float tau, const Scene& s) { return tau > s.cutoff_gt; }
+template <> __device__ __forceinline__ bool tau_alive<double>(double tau, const Scene& s) { return tau > s.cutoff_d; }
 
 template <class R>
 struct RayRun {
     R s[6];      // x, y, z, p_x, p_y, p_z
     R k1[6];     // RHS at s (valid when have_k1)
     R pt, kt, h, tol;
-    float col[3];
-    float tau;
+    R col[3];    // colour and transmittance: float on the float paths, double on the FP64 path
+    R tau;
     int step;    // committed steps (the reference's loop index i)
     int attempt; // attempts spent on the current step
     bool have_k1;
@@ -156,17 +160,26 @@ __device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
     return base * (R(5) - R(4) * t);
 }
 
-// Blackbody colour for the FP64 path (software interpolation, double coordinate).
-__device__ __forceinline__ float3 blackbody_rgb_d(double T, const Scene& sc, uint32_t* err) {
+// Blackbody colour for the FP64 path: software interpolation of the LUT in double.
+__device__ __forceinline__ void blackbody_rgb_d(double T, const Scene& sc, uint32_t* err, double c[3]) {
+    c[0] = c[1] = c[2] = 0.0;
     if (T > (double)sc.lut_max_temp) {
         if (atomicCAS(err, 0u, 1u) == 0u) err[1] = __float_as_uint((float)T);
-        return make_float3(0.0f, 0.0f, 0.0f);
+        return;
     }
-    const double tn = T / (double)sc.lut_max_temp;
-    const double pos = tn * (double)(sc.lut_size - 1);
-    const double u = (pos + 0.5) / (double)sc.lut_size;
-    const float4 c = lut_lerp4<double>(sc.bb_lut, sc.lut_size, u);
-    return make_float3(c.x, c.y, c.z);
+    const int n = sc.lut_size;
+    const double pos = T / (double)sc.lut_max_temp * (double)(n - 1);
+    const double fl = floor(pos);
+    const double flc = fl < -1.0 ? -1.0 : (fl > (double)(n - 1) ? (double)(n - 1) : fl);
+    int i0 = fl == fl ? (int)flc : 0;
+    int i1 = i0 + 1;
+    i0 = i0 < 0 ? 0 : i0;
+    i1 = i1 > n - 1 ? n - 1 : i1;
+    const double w = pos - fl;
+    const float4 a = __ldg(sc.bb_lut + i0), b = __ldg(sc.bb_lut + i1);
+    c[0] = (double)a.x + w * ((double)b.x - (double)a.x);
+    c[1] = (double)a.y + w * ((double)b.y - (double)a.y);
+    c[2] = (double)a.z + w * ((double)b.z - (double)a.z);
 }
 
 // Root of y(t) = 0 on the dense output (stated physics): safeguarded Newton with bisection
@@ -196,13 +209,14 @@ __device__ __forceinline__ R crossing_root(R y0, R y1, R k1, R k3, R k4, R k5, R
 // (cuda/kerr_trace.cuh:167-228): Novikov-Thorne disk test, redshift g, temperature from the disk
 // LUT (with FBM modulation), blackbody colour and alpha compositing into col / tau.
 template <class R, int MODE>
-__device__ __forceinline__ void shade_hit(const R* hit, R pt, R kt, float* col, float& tau, const Scene& sc,
+__device__ __forceinline__ void shade_hit(const R* hit, R pt, R kt, R* col, R& tau, const Scene& sc,
                                           uint32_t* err, Tally* tl) {
     using O = Ops<R>;
     const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
     const R xh = hit[0], zh = hit[2], pxh = hit[3], pyh = hit[4], pzh = hit[5];
     R rh = ks_radius<R>(xh, R(0), zh, aa);
-    const R r_in = (R)sc.disk_inner, r_out = (R)sc.disk_outer;
+    const R r_in = sizeof(R) == 8 ? (R)sc.disk_inner_d : (R)sc.disk_inner;
+    const R r_out = sizeof(R) == 8 ? (R)sc.disk_outer_d : (R)sc.disk_outer;
     if (!(rh >= r_in && rh <= r_out)) return;
     const R sqM = O::sqrt_rn(M), rs = O::sqrt_rn(rh);
     const R disc = R(1) - R(3) * M / rh + R(2) * a * sqM / (rh * rs);
@@ -229,7 +243,8 @@ __device__ __forceinline__ void shade_hit(const R* hit, R pt, R kt, float* col, 
         else if (MODE == 2) sampled = lut_tex_model1(sc.disk_lut, sc.lut_size, u);
         else sampled = lut_lerp1<float>(sc.disk_lut, sc.lut_size, u);
     } else {
-        sampled = lut_lerp1<double>(sc.disk_lut, sc.lut_size, u);
+        sampled = sc.disk_lut_d ? lut_lerp1<double, double>(sc.disk_lut_d, sc.lut_size, u)
+                                : lut_lerp1<double>(sc.disk_lut, sc.lut_size, u);
     }
     // CONFIG_DISK_TEMPERATURE_SCALE is a double literal in the reference: the product is double
     double Td = sc.temp_scale * (double)sampled * (double)g;
@@ -268,14 +283,15 @@ __device__ __forceinline__ void shade_hit(const R* hit, R pt, R kt, float* col, 
             col[2] += c.z * alpha * tau;
             tau *= (1.0f - alpha);
         } else {
-            const float3 c = blackbody_rgb_d(T, sc, err);
-            const double luma = 0.2126 * (double)c.x + 0.7152 * (double)c.y + 0.0722 * (double)c.z;
+            double c[3];
+            blackbody_rgb_d(T, sc, err, c);
+            const double luma = 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2];
             const double luma_s = luma / sc.wl_step;
             const double alpha = 1.0 - exp(-luma_s * 0.5);
-            col[0] += (float)((double)c.x * alpha * (double)tau);
-            col[1] += (float)((double)c.y * alpha * (double)tau);
-            col[2] += (float)((double)c.z * alpha * (double)tau);
-            tau *= (float)(1.0 - alpha);
+            col[0] += c[0] * alpha * tau;
+            col[1] += c[1] * alpha * tau;
+            col[2] += c[2] * alpha * tau;
+            tau *= 1.0 - alpha;
         }
     }
 }
@@ -391,14 +407,14 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
         hamilton_rhs<R, EXACT>(ry.s, ry.pt, a, aa, M, ke);
         if (COUNT) tl.rhs++;
         const R inv = O::rsq(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
-        const float sky = sky_value<R>(ke[0] * inv, ke[1] * inv, ke[2] * inv, ry.tau, sc);
+        const R sky = sky_value<R>(ke[0] * inv, ke[1] * inv, ke[2] * inv, ry.tau, sc);
         ry.col[0] += sky;
         ry.col[1] += sky;
         ry.col[2] += sky;
         return true;
     }
     ry.step++;
-    return !(ry.step < sc.max_steps && ry.tau > sc.cutoff_gt);
+    return !(ry.step < sc.max_steps && tau_alive<R>(ry.tau, sc));
 }
 
 // =========================================================================================

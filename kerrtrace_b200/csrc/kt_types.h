@@ -46,6 +46,10 @@ struct Scene {
     float noise_phase;
     float zone_r;        // mixed precision: FP64 update below this Kerr-Schild radius
     int zone_err64;      // mixed precision: FP64 error norm in the zone (tolerance below 3e-7)
+    // FP64 path: disk radii, and optionally a double disk LUT (the differentiable trace sets
+    // them from double parameters; otherwise they are the float values and the float LUT)
+    double disk_inner_d, disk_outer_d;
+    const double* disk_lut_d;
     float spec_tol_floor;// stated physics: tolerance never drops below base_tol * this
     int width, height;
 };

@@ -178,6 +178,40 @@ def c4_jobs(seed: int = 123, scale: int = 1) -> list[tuple[KtConfig, KtCamera]]:
     return jobs
 
 
+C5_TARGET = (0.7, 60.0, 1.0, 25.0)   # spin, inclination (deg), temperature scale, disk outer radius
+C5_START = (0.5, 50.0, 0.8, 20.0)
+
+
+def c5(size: int = 512, precision: int = 0):
+    """Differentiable inverse problem: 512x512, FOV 30, r_obs 50, stated physics, spp 1, no
+    noise, tolerance 1e-6.  Returns (KtConfig, KtDiffView); theta = C5_TARGET renders the
+    target, C5_START is the starting point.  The view's base temperature scale puts the
+    disk-LUT peak at 1e4 K at the target's spin and r_out, so theta's temperature scale is a
+    plain multiplier."""
+    from . import KtDiffView
+    c = config_default()
+    c.width = c.height = size
+    c.spp = 1
+    c.mode, c.precision = 1, precision
+    c.spin, c.mass = C5_TARGET[0], 1.0
+    c.tolerance = 1e-6
+    c.initial_step = 0.1
+    c.max_steps = 20000
+    c.max_attempts = 3
+    c.escape_radius = 1000.0
+    c.horizon_epsilon = 0.01
+    c.disk_outer_radius = C5_TARGET[3]
+    c.lut_size = 1024
+    c.wavelength_start, c.wavelength_end, c.wavelength_step = 380.0, 720.0, 10.0
+    c.lut_max_temp = 1e5
+    c.disk_temperature_scale = _peak_scale(c, 1e4)
+    c.exposure_scale = 3e-3
+    c.noise_enabled = 0
+    c.bloom_enabled = 0
+    view = KtDiffView(50.0, 0.0, 30.0, float(c.disk_temperature_scale))
+    return c, view
+
+
 SCENES = {"c1": c1, "c2": c2, "t1": t1, "t2": t2, "c3": c3}
 
 
