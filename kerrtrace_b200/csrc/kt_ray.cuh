@@ -197,7 +197,9 @@ __device__ __forceinline__ R crossing_root(R y0, R y1, R k1, R k3, R k4, R k5, R
         if ((yt < R(0)) == neg0) lo = t; else hi = t;
         const R dyt = dense_slope<R>(y0, y1, k1, k3, k4, k5, k6, k7, h, t);
         R tn = dyt != R(0) ? t - yt / dyt : R(0.5) * (lo + hi);
-        if (!(tn > lo && tn < hi)) tn = R(0.5) * (lo + hi);
+        // a converged update (tn == t on the bracket end) is kept: the step is then 0 and the
+        // loop ends; only steps leaving the bracket bisect
+        if (!(tn >= lo && tn <= hi)) tn = R(0.5) * (lo + hi);
         const R step = O::absr(tn - t);
         t = tn;
         if (step <= lit<R>(1e-7f, 1e-15)) break;

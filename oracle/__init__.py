@@ -86,6 +86,8 @@ def olib() -> C.CDLL:
         L.kto_dense.restype = C.c_double
         L.kto_dense_slope.argtypes = [C.c_void_p, C.c_double]
         L.kto_dense_slope.restype = C.c_double
+        L.kto_crossing_root.argtypes = [C.c_void_p, C.c_double]
+        L.kto_crossing_root.restype = C.c_double
         L.kto_fbm.argtypes = [C.c_double, C.c_double, C.c_int, C.c_uint32]
         L.kto_fbm.restype = C.c_double
         L.kto_aces.argtypes = [C.c_double]

@@ -203,6 +203,28 @@ template <class T> T dense_slope(T y0, T y1, T k1, T k3, T k4, T k5, T k6, T k7,
     return (q2 + q3) - T(2) * t * (q3 - q4 - q5) - T(3) * t * t * (q4 + T(2) * q5) + T(4) * t * t * t * q5;
 }
 
+// Root of y(t) = 0 on the dense output (stated physics): Newton from the secant guess t,
+// safeguarded by the bracket [lo, hi] that the iterates keep; an update that leaves the bracket
+// is replaced by bisection.  A converged update (tn == t, which may sit on the bracket end) is
+// kept: the step is then 0 and the loop ends.
+template <class T>
+T crossing_root(T y0, T y1, T k1, T k3, T k4, T k5, T k6, T k7, T hs, T t) {
+    T lo = 0, hi = 1;
+    const bool neg0 = y0 < 0;
+    for (int it = 0; it < 12; ++it) {
+        const T yt = dense<T>(y0, y1, k1, k3, k4, k5, k6, k7, hs, t);
+        if (yt == 0) break;
+        if ((yt < 0) == neg0) lo = t; else hi = t;
+        const T dyt = dense_slope<T>(y0, y1, k1, k3, k4, k5, k6, k7, hs, t);
+        T tn = dyt != 0 ? t - yt / dyt : T(0.5) * (lo + hi);
+        if (!(tn >= lo && tn <= hi)) tn = T(0.5) * (lo + hi);
+        const T stp = std::fabs(tn - t);
+        t = tn;
+        if (stp <= M<T>::lit(1e-7f, 1e-15)) break;
+    }
+    return t;
+}
+
 template <class T> T fade(T t) { return t * t * t * (t * (t * T(6) - T(15)) + T(10)); }
 template <class T> T lerp_(T a, T b, T t) { return a + t * (b - a); }
 template <class T> void lattice_grad(int ix, int iy, uint32_t seed, T* gx, T* gy) {
@@ -460,21 +482,7 @@ RayResult trace_ray(const kto_scene& s, const Derived& dv, const float dirf[3], 
                 const T y0 = prev[1], y1 = st[1];
                 T t = (y0 - y1) != T(0) ? y0 / (y0 - y1) : T(0.5);
                 t = std::min(std::max(t, T(0)), T(1));
-                if (s.mode == 1) {
-                    T lo = 0, hi = 1;
-                    const bool neg0 = y0 < 0;
-                    for (int it = 0; it < 12; ++it) {
-                        const T yt = dense<T>(y0, y1, K1[1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], hs, t);
-                        if (yt == 0) break;
-                        if ((yt < 0) == neg0) lo = t; else hi = t;
-                        const T dyt = dense_slope<T>(y0, y1, K1[1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], hs, t);
-                        T tn = dyt != 0 ? t - yt / dyt : T(0.5) * (lo + hi);
-                        if (!(tn > lo && tn < hi)) tn = T(0.5) * (lo + hi);
-                        const T stp = std::fabs(tn - t);
-                        t = tn;
-                        if (stp <= M<T>::lit(1e-7f, 1e-15)) break;
-                    }
-                }
+                if (s.mode == 1) t = crossing_root<T>(y0, y1, K1[1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], hs, t);
                 T hp[6];
                 for (int c = 0; c < 6; ++c) hp[c] = dense<T>(prev[c], st[c], K1[c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c], hs, t);
                 const T xh = hp[0], zh = hp[2];
@@ -780,6 +788,9 @@ void kto_rhs_reference(const double* st, double pt, double a, double mass, doubl
 }
 double kto_dense(const double* q, double t) { return dense<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t); }
 double kto_dense_slope(const double* q, double t) { return dense_slope<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t); }
+double kto_crossing_root(const double* q, double t0) {
+    return crossing_root<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t0);
+}
 double kto_fbm(double u, double v, int octaves, uint32_t seed) { return fbm<double>(u, v, octaves, seed); }
 double kto_aces(double x) { return aces(x); }
 double kto_srgb(double x) { return srgb(x); }

@@ -187,6 +187,27 @@ def test_dense_output_interpolates_the_step():
         assert (d(t + 1e-6) - d(t - 1e-6)) / 2e-6 == pytest.approx(ds(t), rel=1e-5, abs=1e-7)
 
 
+def test_crossing_root_converges():
+    """The safeguarded Newton root of y(t) = 0 on the dense output lands on the root (|y| at
+    rounding level) for steps whose y changes sign, including the case where the last Newton
+    update rounds to the bracket end (which must end the iteration, not restart a bisection)."""
+    rng = np.random.default_rng(11)
+    worst = 0.0
+    for _ in range(3000):
+        q = np.zeros(9)
+        q[0] = rng.uniform(0.05, 3.0) * rng.choice([-1.0, 1.0])   # y0
+        q[1] = -np.sign(q[0]) * rng.uniform(0.05, 3.0)            # y1: opposite sign
+        q[8] = rng.uniform(0.05, 1.0)                              # h
+        slope = (q[1] - q[0]) / q[8]
+        q[2:8] = slope * (1.0 + 0.05 * rng.normal(size=6))         # stage slopes near the chord
+        t0 = q[0] / (q[0] - q[1])
+        t = olib().kto_crossing_root(q.ctypes.data, t0)
+        assert 0.0 <= t <= 1.0
+        y = olib().kto_dense(q.ctypes.data, t)
+        worst = max(worst, abs(y) / max(abs(q[0]), abs(q[1])))
+    assert worst < 1e-12, worst
+
+
 def test_dense_output_accuracy_on_a_ray():
     """Interpolating inside one DP5 step agrees with re-integrating to that point (4th order)."""
     st, pt = null_init([10.0, 1.0, 2.0], [-1.0, 0.1, -0.2], 0.9)
