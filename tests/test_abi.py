@@ -199,3 +199,15 @@ def test_invalid_configs_rejected_before_device(kt):
     c = cfg.copy()
     c.mode, c.precision = kt.MODE_REF, kt.PREC_FP64
     assert kt.lib().kt_context_create(C.byref(c), 0, C.byref(C.c_void_p())) == kt.KT_ERR_INVALID_ARG
+
+
+def test_diff_rejects_unsupported_configurations(kt):
+    """The differentiable trace needs stated physics, spp 1, noise off and FP32 or FP64; the checks
+    run before any device work."""
+    from kerrtrace_b200 import workloads
+    cfg, view = workloads.c5(32, kt.PREC_FP64)
+    for field, value in (("mode", kt.MODE_REF), ("spp", 2), ("noise_enabled", 1), ("precision", kt.PREC_MIXED)):
+        c = cfg.copy()
+        setattr(c, field, value)
+        with pytest.raises(kt.KtError):
+            kt.Diff(c, view)

@@ -1,0 +1,144 @@
+"""Differentiable trace (kt_diff_*) on the GPU: the recorded forward is the renderer's image,
+the frozen-step replay reproduces it, and the discrete adjoint matches central differences of
+the frozen-step model (FP64, double images) in total and pixel by pixel; the FP32 adjoint tracks
+the FP64 one.  Scene: the inverse-problem workload at 64x64, at its starting parameters."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import kerrtrace_b200 as kt
+from kerrtrace_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+SIZE = 64
+THETA = list(workloads.C5_START)
+EPS = [1e-5, 1e-4, 1e-5, 1e-4]  # spin, inclination (deg), temperature scale, r_out
+NAMES = ["spin", "inclination", "temperature scale", "r_out"]
+
+
+def make(prec):
+    cfg, view = workloads.c5(SIZE, prec)
+    return cfg, view, kt.Diff(cfg, view)
+
+
+def forward(torch, d, theta):
+    n = SIZE * SIZE
+    hdr = torch.zeros((n, 4), device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    d.forward(theta, hdr.data_ptr(), err.data_ptr())
+    torch.cuda.synchronize()
+    assert int(err[0]) == 0
+    return hdr
+
+
+def replay(torch, d, theta):
+    n = SIZE * SIZE
+    hdr = torch.zeros((n, 4), device="cuda")
+    h64 = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    flags = torch.zeros(n, dtype=torch.int32, device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    d.replay(theta, hdr.data_ptr(), flags.data_ptr(), err.data_ptr(), hdr64_ptr=h64.data_ptr())
+    torch.cuda.synchronize()
+    return hdr, h64, flags.bool()
+
+
+def backward(torch, d, w):
+    g = torch.zeros(4, dtype=torch.float64, device="cuda")
+    d.backward(w.data_ptr(), g.data_ptr())
+    torch.cuda.synchronize()
+    return g.cpu().numpy()
+
+
+def central_differences(torch, d):
+    """Richardson-extrapolated central differences per pixel and parameter, and the mask of
+    pixels they cannot resolve: event flips under the perturbation, and pixels whose
+    differences at eps and eps/2 disagree (a LUT cell edge or a sky-line edge inside the step)."""
+    n = SIZE * SIZE
+    mask = torch.zeros(n, dtype=torch.bool, device="cuda")
+    fd = []
+    for j in range(4):
+        img = {}
+        for sgn in (1, -1):
+            for k in (1, 2):
+                t2 = list(THETA)
+                t2[j] += sgn * EPS[j] / k
+                _, h64, flags = replay(torch, d, t2)
+                img[(sgn, k)] = h64
+                mask |= flags
+        f1 = (img[(1, 1)] - img[(-1, 1)]) / (2 * EPS[j])
+        f2 = (img[(1, 2)] - img[(-1, 2)]) / EPS[j]
+        mask |= ((f1 - f2).abs() > 1e-3 * f2.abs() + 1e-7 * f2.abs().max()).any(dim=1)
+        fd.append((4 * f2 - f1) / 3)
+    return fd, mask
+
+
+def test_record_is_the_renderer_image_and_replay_reproduces_it(cuda):
+    for prec in (kt.PREC_FP32, kt.PREC_FP64):
+        cfg, view, d = make(prec)
+        hdr = forward(cuda, d, THETA)
+        h2, _, flags = replay(cuda, d, THETA)
+        assert cuda.equal(h2.view(cuda.int32), hdr.view(cuda.int32))
+        assert not bool(flags.any())
+        info = d.info()
+        assert info.overflow_rays == 0 and 0 < info.segments_used <= info.segments_capacity
+        if prec == kt.PREC_FP32:
+            c = cfg.copy()
+            c.spin, c.disk_outer_radius = THETA[0], THETA[3]
+            c.disk_temperature_scale = view.base_temperature_scale * THETA[2]
+            cam, _ = kt.diff_orbit_camera(view.observer_r, THETA[1], view.azimuth_deg, view.fov_deg)
+            ctx = kt.Context(c)
+            h3 = cuda.zeros_like(hdr)
+            err = cuda.zeros(2, dtype=cuda.int32, device="cuda")
+            ctx.trace(cam, h3.data_ptr(), err.data_ptr(), 0, kt.SCHED_PLAIN)
+            cuda.cuda.synchronize()
+            assert cuda.equal(h3.view(cuda.int32), hdr.view(cuda.int32))
+        d.close()
+
+
+def test_fp64_adjoint_matches_central_differences(cuda):
+    _, _, d = make(kt.PREC_FP64)
+    hdr = forward(cuda, d, THETA)
+    fd, mask = central_differences(cuda, d)
+    lit = hdr[:, :3].sum(1) > 0
+    assert int(mask.sum()) <= 0.02 * int(lit.sum())
+    n = SIZE * SIZE
+    rng = np.random.default_rng(1)
+    w = cuda.tensor((rng.standard_normal((n, 4)) + 1.0).astype(np.float32), device="cuda")
+    w[:, 3] = 0
+    w[mask] = 0
+    g = backward(cuda, d, w)
+    for j in range(4):
+        ref = float((fd[j] * w[:, :3].double()).sum())
+        assert abs(g[j] - ref) <= 1e-4 * abs(ref), (NAMES[j], g[j], ref)
+    # pixel by pixel (one-hot cotangents)
+    cand = np.flatnonzero((lit & ~mask).cpu().numpy())
+    pick = np.random.default_rng(2).choice(cand, size=min(40, len(cand)), replace=False)
+    rel = [[] for _ in range(4)]
+    for p in pick:
+        e = cuda.zeros((n, 4), device="cuda")
+        e[p, :3] = 1.0
+        gp = backward(cuda, d, e)
+        for j in range(4):
+            f = float(fd[j][p].sum())
+            rel[j].append(abs(gp[j] - f) / (abs(f) + 1e-6 * float(fd[j].sum(1).abs().max())))
+    for j in range(4):
+        assert np.median(rel[j]) < 1e-6 and np.max(rel[j]) < 1e-3, (NAMES[j], np.median(rel[j]), np.max(rel[j]))
+    d.close()
+
+
+def test_fp32_adjoint_tracks_fp64(cuda):
+    n = SIZE * SIZE
+    rng = np.random.default_rng(4)
+    w = cuda.tensor((rng.standard_normal((n, 4)) + 1.0).astype(np.float32), device="cuda")
+    w[:, 3] = 0
+    g = {}
+    for prec in (kt.PREC_FP64, kt.PREC_FP32):
+        _, _, d = make(prec)
+        forward(cuda, d, THETA)
+        g[prec] = backward(cuda, d, w)
+        d.close()
+    for j in range(3):
+        assert abs(g[kt.PREC_FP32][j] - g[kt.PREC_FP64][j]) <= 2e-3 * abs(g[kt.PREC_FP64][j]), NAMES[j]
+    assert abs(g[kt.PREC_FP32][3] - g[kt.PREC_FP64][3]) <= 5e-2 * abs(g[kt.PREC_FP64][3])
