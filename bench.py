@@ -59,6 +59,7 @@ def parse():
                     help="arithmetic of the main loop (mixed / fp64 need --mode spec)")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--size", default=None, help="WxH override of the scene resolution (same scene otherwise)")
@@ -283,6 +284,86 @@ def batch_leg(local, reps: int) -> dict:
     return out
 
 
+def adjoint_leg(local, reps: int, size: int = 512) -> dict:
+    """The differentiable inverse problem (512^2, FOV 30, r_obs 50, stated physics): L2 loss on
+    linear HDR between the image at the starting parameters and the target image; forward with
+    step records, then the discrete adjoint (VJP) of the loss.  Per precision: forward, backward
+    and adjoint Mrays/s (rays / (forward + backward)), the cost ratio, record memory and the
+    gradient; for FP64 also its agreement with central differences of the frozen-step model
+    (Richardson-extrapolated, double images, unresolvable pixels masked)."""
+    import torch
+
+    import kerrtrace_b200 as kt
+    from kerrtrace_b200 import workloads
+
+    n = size * size
+    out = {"size": size, "rays": n, "theta_start": list(workloads.C5_START), "theta_target": list(workloads.C5_TARGET)}
+    for pname, prec in (("fp32", kt.PREC_FP32), ("fp64", kt.PREC_FP64)):
+        cfg, view = workloads.c5(size, prec)
+        d = kt.Diff(cfg, view, device=local)
+        err = torch.zeros(2, dtype=torch.int32, device="cuda")
+        target = torch.zeros((n, 4), device="cuda")
+        hdr = torch.zeros((n, 4), device="cuda")
+        d.forward(list(workloads.C5_TARGET), target.data_ptr(), err.data_ptr())
+        d.forward(list(workloads.C5_START), hdr.data_ptr(), err.data_ptr())
+        torch.cuda.synchronize()
+        w = 2.0 * (hdr - target)
+        w[:, 3] = 0
+        loss = float(((hdr[:, :3] - target[:, :3]).double() ** 2).sum())
+        g = torch.zeros(4, dtype=torch.float64, device="cuda")
+        tf, tb = [], []
+        for _ in range(reps):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            d.forward(list(workloads.C5_START), hdr.data_ptr(), err.data_ptr())
+            e1.record()
+            d.backward(w.data_ptr(), g.data_ptr())
+            e2.record()
+            torch.cuda.synchronize()
+            tf.append(e0.elapsed_time(e1))
+            tb.append(e1.elapsed_time(e2))
+        f_ms, b_ms = sorted(tf)[len(tf) // 2], sorted(tb)[len(tb) // 2]
+        info = d.info()
+        r = {"forward_ms": round(f_ms, 3), "backward_ms": round(b_ms, 3),
+             "forward_mrays_s": round(n / f_ms / 1e3, 2), "adjoint_mrays_s": round(n / (f_ms + b_ms) / 1e3, 2),
+             "cost_ratio": round((f_ms + b_ms) / f_ms, 2), "loss": loss, "grad": g.cpu().tolist(),
+             "record_mb": round(info.record_bytes / 2**20, 2), "diff_device_mb": round(info.device_bytes / 2**20, 1),
+             "overflow_rays": int(info.overflow_rays)}
+        if prec == kt.PREC_FP64:
+            th = list(workloads.C5_START)
+            eps = [1e-5, 1e-4, 1e-5, 1e-4]
+            mask = torch.zeros(n, dtype=torch.bool, device="cuda")
+            fd = []
+            for j in range(4):
+                img = {}
+                for sgn in (1, -1):
+                    for k in (1, 2):
+                        t2 = list(th)
+                        t2[j] += sgn * eps[j] / k
+                        hh = torch.zeros((n, 4), device="cuda")
+                        h64 = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+                        fl = torch.zeros(n, dtype=torch.int32, device="cuda")
+                        d.replay(t2, hh.data_ptr(), fl.data_ptr(), err.data_ptr(), hdr64_ptr=h64.data_ptr())
+                        torch.cuda.synchronize()
+                        img[(sgn, k)] = h64
+                        mask |= fl.bool()
+                f1 = (img[(1, 1)] - img[(-1, 1)]) / (2 * eps[j])
+                f2 = (img[(1, 2)] - img[(-1, 2)]) / eps[j]
+                mask |= ((f1 - f2).abs() > 1e-3 * f2.abs() + 1e-7 * f2.abs().max()).any(dim=1)
+                fd.append((4 * f2 - f1) / 3)
+            wm = w.clone()
+            wm[mask] = 0
+            d.backward(wm.data_ptr(), g.data_ptr())
+            torch.cuda.synchronize()
+            ga = g.cpu().tolist()
+            ref = [float((fd[j] * wm[:, :3].double()).sum()) for j in range(4)]
+            r["fd_check"] = {"eps": eps, "masked_pixels": int(mask.sum()), "adjoint": ga, "central_differences": ref,
+                             "rel_err": [abs(ga[j] - ref[j]) / max(abs(ref[j]), 1e-300) for j in range(4)]}
+        out[pname] = r
+        d.close()
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -402,6 +483,8 @@ def run_ours(args, rank, world, local):
         line["precision"] = precision_leg(cfg, cam, local, max(3, args.steps))
     if rank == 0 and world == 1 and not args.no_batch:
         line["batch"] = batch_leg(local, 3)
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(local, max(3, args.steps))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, cam, args.cpu_seconds)
     if rank == 0:
