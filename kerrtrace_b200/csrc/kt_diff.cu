@@ -10,9 +10,10 @@
 //                                  (max_attempts = 1 in the scene), at new parameters; flags the
 //                                  rays whose events differ from the record.  Central
 //                                  differences of the frozen-step model use it.
-//   diff_backward_kernel<R>        discrete adjoint.  Per ray, from the last segment back: replay
-//                                  the segment forward (states before each step, crossings), then
-//                                  reverse each step:
+//   diff_backward_kernel<R>        discrete adjoint.  Per ray, from the last segment back: sweep
+//                                  the segment forward from its checkpoint (states and stages of
+//                                  each step, transmittance at the crossings the record marks as
+//                                  shaded, kept in local memory), then reverse each step:
 //     * crossing: the hit is the dense-output point at the root t* of y(t) = 0; its shading
 //       (disk test, redshift, LUT temperature, blackbody, alpha) is differentiated with duals
 //       in the hit state, p_t, k_t, spin, temperature scale and r_out; the transmittance chain
@@ -27,6 +28,8 @@
 //   inclination (the camera's inclination tangent comes from the host).
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "kt_diff.h"
 #include "kt_dual.cuh"
@@ -121,87 +124,100 @@ __device__ __forceinline__ void rhs_vjp(const R* Y, const R* l, R pt, R a, R aa,
 // Tangent slots of the shading duals.
 enum : int { kSX = 0, kSPt = 6, kSKt = 7, kSA = 8, kSTs = 9, kSRo = 10, kSN = 11 };
 
-// Disk shading of hit state X (shade_hit<R, 1> without noise) on duals: returns false where the
-// hit is not shaded; else the blackbody colour c and the opacity alpha with their derivatives.
-template <class R>
-__device__ bool shade_dual(const R* X, R pt, R kt, const Scene& sc, const DiffLut& dl, Dual<R, kSN>* c3,
-                           Dual<R, kSN>& alpha) {
-    using D = Dual<R, kSN>;
-    using O = Ops<D>;
-    D h[6];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) h[c] = D::seed(X[c], kSX + c);
-    const D Dpt = D::seed(pt, kSPt), Dkt = D::seed(kt, kSKt);
-    const D a = D::seed(sc_a<R>(sc), kSA);
-    const D aa = a * a;
+// Value / tangent helpers shared by the plain and the dual evaluation of the shading.
+template <class R> __device__ __forceinline__ R val(R x) { return x; }
+template <class R, int N> __device__ __forceinline__ R val(const Dual<R, N>& x) { return x.v; }
+template <class T, class R>
+__device__ __forceinline__ T seeded(R x, int slot) {
+    if constexpr (std::is_same<T, R>::value) return x;
+    else return T::seed(x, slot);
+}
+// a scene input with its derivatives in the shading slots (plain value for T = R)
+template <class T, class R>
+__device__ __forceinline__ T with_tangent(R x, int slot, R dx) {
+    T r(x);
+    if constexpr (!std::is_same<T, R>::value) r.d[slot] = dx;
+    return r;
+}
+
+// Disk shading of hit state X (shade_hit<R, 1> without noise), on plain values (T = R) or on
+// duals in the hit state, p_t, k_t, spin, temperature scale and r_out (T = Dual<R, kSN>):
+// returns false where the hit is not shaded; else the blackbody colour c and the opacity alpha.
+template <class R, class T>
+__device__ bool shade_eval(const R* X, R pt, R kt, const Scene& sc, const DiffLut& dl, T* c3, T& alpha) {
+    using O = Ops<T>;
+    const T xh = seeded<T>(X[0], kSX + 0), zh = seeded<T>(X[2], kSX + 2);
+    const T pxh = seeded<T>(X[3], kSX + 3), pzh = seeded<T>(X[5], kSX + 5);
+    const T Dpt = seeded<T>(pt, kSPt), Dkt = seeded<T>(kt, kSKt);
+    const T a = seeded<T>(sc_a<R>(sc), kSA);
+    const T aa = a * a;
     const R M = sc_M<R>(sc);
-    D r_in(sizeof(R) == 8 ? (R)sc.disk_inner_d : (R)sc.disk_inner);
-    r_in.d[kSA] = (R)dl.dr_in_da;
-    const D r_out = D::seed(sizeof(R) == 8 ? (R)sc.disk_outer_d : (R)sc.disk_outer, kSRo);
-    const D xh = h[0], zh = h[2], pxh = h[3], pzh = h[5];
-    const D rh = ks_radius<D>(xh, D(R(0)), zh, aa);
-    if (!(rh >= r_in && rh <= r_out)) return false;
+    const T r_in = with_tangent<T>(sizeof(R) == 8 ? (R)sc.disk_inner_d : (R)sc.disk_inner, kSA, (R)dl.dr_in_da);
+    const T r_out = seeded<T>(sizeof(R) == 8 ? (R)sc.disk_outer_d : (R)sc.disk_outer, kSRo);
+    const T rh = ks_radius<T>(xh, T(R(0)), zh, aa);
+    if (!(val(rh) >= val(r_in) && val(rh) <= val(r_out))) return false;
     const R sqM = Ops<R>::sqrt_rn(M);
-    const D rs = O::sqrt_rn(rh);
-    const D disc = R(1) - R(3) * M / rh + R(2) * sqM * a / (rh * rs);
-    if (!(disc.v > R(0))) return false;
-    const D omega = -sqM / (rh * rs + a * sqM);
-    const D r2h = rh * rh;
-    const D inv = R(1) / (r2h + aa);
-    const D lx = (rh * xh - a * zh) * inv;
-    const D lz = (rh * zh + a * xh) * inv;
-    const D ldotp = O::fma(lx, pxh, lz * pzh);
-    const D ldotxi = lx * zh - lz * xh;
-    const D Hk = M * rh * r2h / (r2h * r2h);
-    const D L = (zh * pxh - xh * pzh) + R(2) * Hk * ldotxi * (ldotp + Dkt);
-    const D energy = -Dpt;
-    const D l_over_e = L / energy;
-    const D g = R(1) / (O::rsq(disc) * (R(1) - omega * l_over_e));
-    const D span = r_out - r_in;
-    const D u = span.v > R(0) ? (rh - r_in) / span : D(R(0));
+    const T rs = O::sqrt_rn(rh);
+    const T disc = R(1) - R(3) * M / rh + R(2) * sqM * a / (rh * rs);
+    if (!(val(disc) > R(0))) return false;
+    const T omega = -sqM / (rh * rs + a * sqM);
+    const T r2h = rh * rh;
+    const T inv = R(1) / (r2h + aa);
+    const T lx = (rh * xh - a * zh) * inv;
+    const T lz = (rh * zh + a * xh) * inv;
+    const T ldotp = O::fma(lx, pxh, lz * pzh);
+    const T ldotxi = lx * zh - lz * xh;
+    const T Hk = M * rh * r2h / (r2h * r2h);
+    const T L = (zh * pxh - xh * pzh) + R(2) * Hk * ldotxi * (ldotp + Dkt);
+    const T energy = -Dpt;
+    const T l_over_e = L / energy;
+    const T g = R(1) / (O::rsq(disc) * (R(1) - omega * l_over_e));
+    const T span = r_out - r_in;
+    const T u = val(span) > R(0) ? (rh - r_in) / span : T(R(0));
     // disk LUT, software linear fetch (lut_lerp1); the entries carry their spin / r_out tangents
     const int n = sc.lut_size;
-    const D x = u * R(n) - R(0.5);
-    const R fl = floor(x.v);
+    const T x = u * R(n) - R(0.5);
+    const R fl = floor(val(x));
     const R flc = fl < R(-1) ? R(-1) : (fl > R(n - 1) ? R(n - 1) : fl);
     int i0 = fl == fl ? (int)flc : 0;
     int i1 = i0 + 1;
     i0 = i0 < 0 ? 0 : i0;
     i1 = i1 > n - 1 ? n - 1 : i1;
     const bool lut_d = sizeof(R) == 8 && sc.disk_lut_d;
-    D v0(lut_d ? (R)__ldg(sc.disk_lut_d + i0) : (R)__ldg(sc.disk_lut + i0));
-    D v1(lut_d ? (R)__ldg(sc.disk_lut_d + i1) : (R)__ldg(sc.disk_lut + i1));
-    v0.d[kSA] = (R)__ldg(dl.dlut_da + i0);
-    v1.d[kSA] = (R)__ldg(dl.dlut_da + i1);
-    v0.d[kSRo] = (R)__ldg(dl.dlut_dro + i0);
-    v1.d[kSRo] = (R)__ldg(dl.dlut_dro + i1);
-    const D w = x - fl;
-    const D sampled = v0 + w * (v1 - v0);
-    D ts((R)sc.temp_scale);
-    ts.d[kSTs] = (R)dl.dtemp_ds;
-    const D T = ts * sampled * g;
-    if (!(Ops<R>::isfiniter(T.v) && T.v > R(0))) return false;
+    T v0 = with_tangent<T>(lut_d ? (R)__ldg(sc.disk_lut_d + i0) : (R)__ldg(sc.disk_lut + i0), kSA,
+                           (R)__ldg(dl.dlut_da + i0));
+    T v1 = with_tangent<T>(lut_d ? (R)__ldg(sc.disk_lut_d + i1) : (R)__ldg(sc.disk_lut + i1), kSA,
+                           (R)__ldg(dl.dlut_da + i1));
+    if constexpr (!std::is_same<T, R>::value) {
+        v0.d[kSRo] = (R)__ldg(dl.dlut_dro + i0);
+        v1.d[kSRo] = (R)__ldg(dl.dlut_dro + i1);
+    }
+    const T w = x - fl;
+    const T sampled = v0 + w * (v1 - v0);
+    const T ts = with_tangent<T>((R)sc.temp_scale, kSTs, (R)dl.dtemp_ds);
+    const T T_ = ts * sampled * g;
+    if (!(Ops<R>::isfiniter(val(T_)) && val(T_) > R(0))) return false;
     // blackbody LUT (blackbody_rgb<1> / blackbody_rgb_d): linear in T between two entries
-    if (T.v > (R)sc.lut_max_temp) {
-        c3[0] = c3[1] = c3[2] = D(R(0));
-        alpha = D(R(0));
+    if (val(T_) > (R)sc.lut_max_temp) {
+        c3[0] = c3[1] = c3[2] = T(R(0));
+        alpha = T(R(0));
         return true;
     }
     const int nb = sc.lut_size;
-    const D pos = T / (R)sc.lut_max_temp * R(nb - 1);
-    const R fb = floor(pos.v);
+    const T pos = T_ / (R)sc.lut_max_temp * R(nb - 1);
+    const R fb = floor(val(pos));
     const R fbc = fb < R(-1) ? R(-1) : (fb > R(nb - 1) ? R(nb - 1) : fb);
     int j0 = fb == fb ? (int)fbc : 0;
     int j1 = j0 + 1;
     j0 = j0 < 0 ? 0 : j0;
     j1 = j1 > nb - 1 ? nb - 1 : j1;
     const float4 ca = __ldg(sc.bb_lut + j0), cb = __ldg(sc.bb_lut + j1);
-    const D wb = pos - fb;
+    const T wb = pos - fb;
     c3[0] = (R)ca.x + wb * (R)(cb.x - ca.x);
     c3[1] = (R)ca.y + wb * (R)(cb.y - ca.y);
     c3[2] = (R)ca.z + wb * (R)(cb.z - ca.z);
-    const D luma = R(0.2126) * c3[0] + R(0.7152) * c3[1] + R(0.0722) * c3[2];
-    const D luma_s = luma / (R)sc.wl_step;
+    const T luma = R(0.2126) * c3[0] + R(0.7152) * c3[1] + R(0.0722) * c3[2];
+    const T luma_s = luma / (R)sc.wl_step;
     alpha = R(1) - O::expr(luma_s * R(-0.5));
     return true;
 }
@@ -403,6 +419,7 @@ __global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const
                         sg->prev = cur;
                         sg->next = -1;
                         sg->n = 0;
+                        sg->hits = 0u;
                         sg->first_step = out.n_steps;
                         sg->tau = ry.tau;
 #pragma unroll
@@ -413,6 +430,7 @@ __global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const
                     }
                 }
                 const R h_used = ry.h;
+                const uint32_t hits0 = tl.hits;
                 const bool done = advance<1, true>(ry, sc, err, tl);
                 if (ry.attempt != 0) continue;  // rejected attempt: the step is retried
                 if (Ops<R>::isnanr(ry.s[1])) {  // frozen: this step is not part of the record
@@ -421,6 +439,7 @@ __global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const
                 }
                 if (rec_ok) {
                     sg->h[in_seg] = h_used;
+                    if (tl.hits != hits0) sg->hits |= 1u << in_seg;
                     sg->n = ++in_seg;
                     out.last_seg = cur;
                     if (in_seg == kSegSteps) in_seg = 0;
@@ -477,11 +496,29 @@ __global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const
 }
 
 // ---- adjoint kernel ----------------------------------------------------------------------------
+// Hit point of step (s -> nx) with stages k: the crossing root of shade_crossing<R, 1>; X the
+// state there, dX its slope in the step fraction.
+template <class R>
+__device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], R h, R* X, R* dX) {
+    const R yv0 = s[1], yv1 = nx[1];
+    const R dy = yv0 - yv1;
+    R t = dy != R(0) ? Ops<R>::fdiv(yv0, dy) : R(0.5);
+    t = Ops<R>::minr(Ops<R>::maxr(t, R(0)), R(1));
+    t = crossing_root<R>(yv0, yv1, k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], h, t);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        X[c] = dense_eval<R>(s[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c], h, t);
+        if (dX) dX[c] = dense_slope<R>(s[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c], h, t);
+    }
+    return t;
+}
+
 template <class R>
 __global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, const Camera cam, const CameraD camd,
                                                            const CameraD dcamd, const DiffRecRaw rec, const DiffLut dl,
                                                            const float4* __restrict__ dl_dhdr,
-                                                           double* __restrict__ grad, uint32_t* __restrict__ err) {
+                                                           double* __restrict__ grad) {
+    using C = DP<R>;
     const unsigned n_px = (unsigned)sc.width * (unsigned)sc.height;
     const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
     double g[4] = {0.0, 0.0, 0.0, 0.0};
@@ -502,40 +539,44 @@ __global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, cons
             R ls[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};  // adjoint of the current state
             R lpt = R(0), lkt = R(0), ga = R(0), gts = R(0), gro = R(0);
             R ltau = rr.term == kTermEscape ? (lc[0] + lc[1] + lc[2]) * (R)rr.sky : R(0);
-            R sj[kSegSteps][6];
-            R tauj[kSegSteps];
-            bool hitj[kSegSteps];
+            R S[kSegSteps][6];          // state before each step of the segment
+            R K[kSegSteps][7][6];       // its stages
+            R TIN[kSegSteps];           // transmittance before a shaded crossing
             for (int si = rr.last_seg; si >= 0;) {
                 const DiffSeg<R>* sg = seg_at<R>(rec, si);
                 const int n = sg->n;
-                // replay the segment: states before each step and its shaded crossings
-                RayRun<R> ry;
+                const unsigned hits = sg->hits;
+                // forward sweep: states, stages, transmittance at the shaded crossings
+                {
+                    R s[6];
 #pragma unroll
-                for (int c = 0; c < 6; ++c) ry.s[c] = sg->s[c];
-                ry.pt = pt;
-                ry.kt = kt;
-                ry.tol = R(0);
-                ry.col[0] = ry.col[1] = ry.col[2] = R(0);
-                ry.tau = sg->tau;
-                ry.step = sg->first_step;
-                ry.attempt = 0;
-                ry.have_k1 = false;
-                Tally tl;
-                tl.clear();
-                for (int j = 0; j < n; ++j) {
+                    for (int c = 0; c < 6; ++c) s[c] = sg->s[c];
+                    R tau = sg->tau;
+                    for (int j = 0; j < n; ++j) {
+                        R nx[6];
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) sj[j][c] = ry.s[c];
-                    tauj[j] = ry.tau;
-                    const uint32_t hits0 = tl.hits;
-                    ry.h = sg->h[j];
-                    advance<1, true>(ry, sc, err, tl);
-                    hitj[j] = tl.hits != hits0;
+                        for (int c = 0; c < 6; ++c) S[j][c] = s[c];
+                        dp5_stages<R>(s, sg->h[j], pt, a, aa, M, K[j], nx);
+                        if (hits >> j & 1u) {
+                            R X[6], c3[3], al;
+                            step_hit<R>(s, nx, K[j], sg->h[j], X, nullptr);
+                            TIN[j] = tau;
+                            if (shade_eval<R, R>(X, pt, kt, sc, dl, c3, al)) tau *= R(1) - al;
+                        }
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) s[c] = nx[c];
+                    }
                 }
-                // reverse the segment's steps
+                // reverse sweep
                 for (int j = n - 1; j >= 0; --j) {
                     const R h = sg->h[j];
-                    R k[7][6], nx[6];
-                    dp5_stages<R>(sj[j], h, pt, a, aa, M, k, nx);
+                    const R(*k)[6] = K[j];
+                    const R* s0 = S[j];
+                    R nx[6];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c)
+                        nx[c] = s0[c] + h * (C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] +
+                                             C::b6 * k[5][c]);
                     R ly0[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
                     R ly1[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
                     R dk[7][6];  // adjoints of k1..k7 from the dense output (k2 stays 0)
@@ -543,25 +584,12 @@ __global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, cons
                     for (int i = 0; i < 7; ++i)
 #pragma unroll
                         for (int c = 0; c < 6; ++c) dk[i][c] = R(0);
-                    if (hitj[j]) {
-                        // hit point: the crossing root of shade_crossing<R, 1>
-                        const R* s0 = sj[j];
-                        const R yv0 = s0[1], yv1 = nx[1];
-                        const R dy = yv0 - yv1;
-                        R t = dy != R(0) ? Ops<R>::fdiv(yv0, dy) : R(0.5);
-                        t = Ops<R>::minr(Ops<R>::maxr(t, R(0)), R(1));
-                        t = crossing_root<R>(yv0, yv1, k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], h, t);
+                    if (hits >> j & 1u) {
                         R X[6], dX[6];
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) {
-                            X[c] = dense_eval<R>(s0[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c],
-                                                 h, t);
-                            dX[c] = dense_slope<R>(s0[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c],
-                                                   k[6][c], h, t);
-                        }
+                        const R t = step_hit<R>(s0, nx, k, h, X, dX);
                         Dual<R, kSN> cc[3], al;
-                        if (shade_dual<R>(X, pt, kt, sc, dl, cc, al)) {
-                            const R tin = tauj[j];
+                        if (shade_eval<R, Dual<R, kSN>>(X, pt, kt, sc, dl, cc, al)) {
+                            const R tin = TIN[j];
                             // col += c alpha tau_in ; tau_out = tau_in (1 - alpha)
                             R q[kSN];
 #pragma unroll
@@ -616,20 +644,12 @@ __global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, cons
 #pragma unroll
                     for (int m = 6; m >= 0; --m) {  // stage m + 1
                         R Y[6];
-                        if (m == 6) {
 #pragma unroll
-                            for (int c = 0; c < 6; ++c) Y[c] = nx[c];
-                        } else if (m == 0) {
+                        for (int c = 0; c < 6; ++c) {
+                            R sum = R(0);
 #pragma unroll
-                            for (int c = 0; c < 6; ++c) Y[c] = sj[j][c];
-                        } else {
-#pragma unroll
-                            for (int c = 0; c < 6; ++c) {
-                                R sum = R(0);
-#pragma unroll
-                                for (int jj = 0; jj < m; ++jj) sum += rk_a<R>(m + 1, jj + 1) * k[jj][c];
-                                Y[c] = sj[j][c] + h * sum;
-                            }
+                            for (int jj = 0; jj < m; ++jj) sum += rk_a<R>(m + 1, jj + 1) * k[jj][c];
+                            Y[c] = m == 0 ? s0[c] : s0[c] + h * sum;
                         }
                         bool nz = false;
 #pragma unroll
@@ -704,9 +724,9 @@ cudaError_t launch_diff_backward(const Scene& sc, const Camera& cam, const Camer
     if (n == 0) return cudaSuccess;
     const dim3 grid((n + 127) / 128);
     if (sc.precision == 2)
-        diff_backward_kernel<double><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, err);
+        diff_backward_kernel<double><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad);
     else
-        diff_backward_kernel<float><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, err);
+        diff_backward_kernel<float><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad);
     return cudaGetLastError();
 }
 

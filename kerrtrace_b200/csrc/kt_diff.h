@@ -37,6 +37,8 @@ struct alignas(16) DiffSeg {
     int prev, next;   // neighbours in the ray's list, -1 at the ends
     int n;            // steps in this segment (1..kSegSteps)
     int first_step;   // index of its first step along the ray
+    unsigned hits;    // bit j: step j shaded a disk crossing
+    int pad;
     R tau;            // transmittance at the segment start
     R s[6];           // state at the segment start
     R h[kSegSteps];   // accepted step sizes
