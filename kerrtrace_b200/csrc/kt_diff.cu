@@ -542,10 +542,15 @@ __global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, cons
             R S[kSegSteps][6];          // state before each step of the segment
             R K[kSegSteps][7][6];       // its stages
             R TIN[kSegSteps];           // transmittance before a shaded crossing
-            for (int si = rr.last_seg; si >= 0;) {
+            // the adjoint of the state is zero after the last shaded crossing: start there
+            int si = rr.last_seg;
+            while (si >= 0 && seg_at<R>(rec, si)->hits == 0u) si = seg_at<R>(rec, si)->prev;
+            bool first = true;
+            while (si >= 0) {
                 const DiffSeg<R>* sg = seg_at<R>(rec, si);
-                const int n = sg->n;
                 const unsigned hits = sg->hits;
+                const int n = first ? 32 - __clz((int)hits) : sg->n;
+                first = false;
                 // forward sweep: states, stages, transmittance at the shaded crossings
                 {
                     R s[6];
