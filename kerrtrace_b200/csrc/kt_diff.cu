@@ -513,8 +513,12 @@ __device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], 
     return t;
 }
 
+// Resident 128-thread blocks per SM asked of the compiler for the adjoint kernel.
+template <class R> struct BackMinBlocks { static constexpr int v = 4; };
+template <> struct BackMinBlocks<double> { static constexpr int v = 2; };
+
 template <class R>
-__global__ void __launch_bounds__(128) diff_backward_kernel(const Scene sc, const Camera cam, const CameraD camd,
+__global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel(const Scene sc, const Camera cam, const CameraD camd,
                                                            const CameraD dcamd, const DiffRecRaw rec, const DiffLut dl,
                                                            const float4* __restrict__ dl_dhdr,
                                                            double* __restrict__ grad) {
