@@ -495,6 +495,71 @@ __global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const
     }
 }
 
+// ---- adjoint work order ------------------------------------------------------------------------
+// The backward's cost per ray is the number of steps up to its last shaded crossing, which
+// ranges from a few to hundreds.  Rays are bucketed by that count (two buckets per power of 2,
+// longest first) and the adjoint kernel takes them in bucket order, so that the rays of a warp
+// have similar lengths; rays without a gradient path are left out.
+constexpr int kWorkBuckets = 32;
+
+template <class R>
+__device__ __forceinline__ int backward_bucket(const DiffRecRaw& rec, const DiffRay& rr, float4 dlp) {
+    const bool live = rr.term != kTermNotStarted && rr.term != kTermOverflow && rr.last_seg >= 0 && rr.n_hits > 0 &&
+                      (dlp.x != 0.0f || dlp.y != 0.0f || dlp.z != 0.0f);
+    if (!live) return -1;
+    int si = rr.last_seg;
+    while (si >= 0 && seg_at<R>(rec, si)->hits == 0u) si = seg_at<R>(rec, si)->prev;
+    if (si < 0) return -1;
+    const DiffSeg<R>* sg = seg_at<R>(rec, si);
+    const unsigned w = (unsigned)sg->first_step + (unsigned)(32 - __clz((int)sg->hits));
+    const int lg = (int)(2.0f * __log2f((float)w));
+    return kWorkBuckets - 1 - (lg < 0 ? 0 : (lg > kWorkBuckets - 1 ? kWorkBuckets - 1 : lg));
+}
+
+// bucket of every pixel (-1: no work) and the bucket sizes; ctl[0..31] counts, ctl[32..63] cursors
+template <class R>
+__global__ void __launch_bounds__(256) diff_bucket_kernel(const Scene sc, const DiffRecRaw rec,
+                                                         const float4* __restrict__ dl_dhdr, int* __restrict__ bucket,
+                                                         unsigned* __restrict__ ctl) {
+    __shared__ unsigned hist[kWorkBuckets];
+    if (threadIdx.x < kWorkBuckets) hist[threadIdx.x] = 0u;
+    __syncthreads();
+    const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
+    const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) {
+        const int b = backward_bucket<R>(rec, rec.rays[p], dl_dhdr[p]);
+        bucket[p] = b;
+        if (b >= 0) atomicAdd(&hist[b], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kWorkBuckets && hist[threadIdx.x]) atomicAdd(&ctl[threadIdx.x], hist[threadIdx.x]);
+}
+
+// exclusive scan of the bucket sizes into the cursors; ctl[64] = rays with work
+__global__ void diff_bucket_scan_kernel(unsigned* __restrict__ ctl) {
+    if (threadIdx.x != 0) return;
+    unsigned acc = 0;
+    for (int b = 0; b < kWorkBuckets; ++b) {
+        ctl[kWorkBuckets + b] = acc;
+        acc += ctl[b];
+    }
+    ctl[2 * kWorkBuckets] = acc;
+}
+
+__global__ void __launch_bounds__(256) diff_bucket_scatter_kernel(unsigned n, const int* __restrict__ bucket,
+                                                                 unsigned* __restrict__ ctl,
+                                                                 unsigned* __restrict__ order) {
+    const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = p < n ? bucket[p] : -1;
+    const unsigned peers = __match_any_sync(kFullMask, b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (b >= 0 && lane == leader) base = atomicAdd(&ctl[kWorkBuckets + b], (unsigned)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    if (b >= 0) order[base + (unsigned)__popc(peers & ((1u << lane) - 1u))] = p;
+}
+
 // ---- adjoint kernel ----------------------------------------------------------------------------
 // Hit point of step (s -> nx) with stages k: the crossing root of shade_crossing<R, 1>; X the
 // state there, dX its slope in the step fraction.
@@ -521,12 +586,14 @@ template <class R>
 __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel(const Scene sc, const Camera cam, const CameraD camd,
                                                            const CameraD dcamd, const DiffRecRaw rec, const DiffLut dl,
                                                            const float4* __restrict__ dl_dhdr,
-                                                           double* __restrict__ grad) {
+                                                           double* __restrict__ grad,
+                                                           const unsigned* __restrict__ order,
+                                                           const unsigned* __restrict__ n_work) {
     using C = DP<R>;
-    const unsigned n_px = (unsigned)sc.width * (unsigned)sc.height;
-    const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned u = blockIdx.x * blockDim.x + threadIdx.x;
     double g[4] = {0.0, 0.0, 0.0, 0.0};
-    if (p < n_px) {
+    if (u < *n_work) {
+        const unsigned p = order[u];
         const DiffRay rr = rec.rays[p];
         const float4 dlp = dl_dhdr[p];
         const R fs = (R)sc.final_scale;
@@ -728,14 +795,21 @@ cudaError_t launch_diff_forward(const Scene& sc, const Camera& cam, const Camera
 
 cudaError_t launch_diff_backward(const Scene& sc, const Camera& cam, const CameraD& camd, const CameraD& dcamd,
                                  const DiffRecRaw& rec, const DiffLut& dl, const float4* dl_dhdr, double* grad,
-                                 uint32_t* err, cudaStream_t st) {
+                                 const DiffWork& wk, cudaStream_t st) {
     const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
     if (n == 0) return cudaSuccess;
-    const dim3 grid((n + 127) / 128);
+    cudaError_t e = cudaMemsetAsync(wk.ctl, 0, (2 * kWorkBuckets + 1) * sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    const dim3 g256((n + 255) / 256), g128((n + 127) / 128);
+    if (sc.precision == 2) diff_bucket_kernel<double><<<g256, 256, 0, st>>>(sc, rec, dl_dhdr, wk.bucket, wk.ctl);
+    else diff_bucket_kernel<float><<<g256, 256, 0, st>>>(sc, rec, dl_dhdr, wk.bucket, wk.ctl);
+    diff_bucket_scan_kernel<<<1, 32, 0, st>>>(wk.ctl);
+    diff_bucket_scatter_kernel<<<g256, 256, 0, st>>>(n, wk.bucket, wk.ctl, wk.order);
+    const unsigned* n_work = wk.ctl + 2 * kWorkBuckets;
     if (sc.precision == 2)
-        diff_backward_kernel<double><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad);
+        diff_backward_kernel<double><<<g128, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, wk.order, n_work);
     else
-        diff_backward_kernel<float><<<grid, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad);
+        diff_backward_kernel<float><<<g128, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, wk.order, n_work);
     return cudaGetLastError();
 }
 

@@ -76,11 +76,20 @@ struct CameraD {
 cudaError_t launch_diff_forward(const Scene& sc, const Camera& cam, const CameraD& camd, const DiffRecRaw& rec,
                                 int replay, float4* hdr, double* hdr64, uint32_t* err, uint32_t* flags,
                                 cudaStream_t stream);
+// Scratch of the adjoint's work ordering: bucket and order (one word per pixel each), ctl
+// (kDiffWorkCtl words).
+constexpr int kDiffWorkCtl = 65;
+struct DiffWork {
+    int* bucket;
+    unsigned* order;
+    unsigned* ctl;
+};
+
 // Adjoint: grad[0..3] += d(sum_p dl_dhdr[p] . hdr[p]) / d(spin, inclination in degrees,
 // temperature-scale parameter, disk outer radius).  dcamd = d(camera)/d(inclination in degrees).
 // The float path starts its rays from cam (the renderer's camera), the double path from camd.
 cudaError_t launch_diff_backward(const Scene& sc, const Camera& cam, const CameraD& camd, const CameraD& dcamd,
                                  const DiffRecRaw& rec, const DiffLut& dl, const float4* dl_dhdr, double* grad,
-                                 uint32_t* err, cudaStream_t stream);
+                                 const DiffWork& work, cudaStream_t stream);
 
 }  // namespace ktd

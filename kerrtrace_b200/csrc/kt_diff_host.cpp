@@ -172,7 +172,8 @@ struct kt_diff {
     size_t seg_bytes = 0;
     ktd::DiffRay* rays = nullptr;
     void* segs = nullptr;
-    unsigned* ctl = nullptr;  // [0] pool cursor, [1] overflow count, [2..3] backward's LUT error word
+    unsigned* ctl = nullptr;  // [0] pool cursor, [1] overflow count
+    ktd::DiffWork work{};     // the adjoint's work ordering
     float4* bb = nullptr;     // blackbody LUT (does not depend on theta)
     kt_diff_luts lut_rec, lut_rep;
     // the recorded point
@@ -200,6 +201,9 @@ void destroy(kt_diff* d) {
     cudaFree(d->segs);
     cudaFree(d->ctl);
     cudaFree(d->bb);
+    cudaFree(d->work.bucket);
+    cudaFree(d->work.order);
+    cudaFree(d->work.ctl);
     free_luts(d->lut_rec);
     free_luts(d->lut_rep);
     delete d;
@@ -333,6 +337,9 @@ kt_status kt_diff_create(const kt_config* cfg, const kt_diff_view* view, uint32_
         (e = cudaMalloc(&d->ctl, 4 * sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMemset(d->ctl, 0, 4 * sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMalloc(&d->bb, (size_t)n * sizeof(float4))) != cudaSuccess ||
+        (e = cudaMalloc(&d->work.bucket, (size_t)d->n_px * sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&d->work.order, (size_t)d->n_px * sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMalloc(&d->work.ctl, ktd::kDiffWorkCtl * sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMemcpy(d->bb, bb.data(), bb.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) {
         destroy(d);
         return err_cuda(e, "diff allocation");
@@ -403,9 +410,8 @@ kt_status kt_diff_backward(kt_diff* d, void* stream, const float* dl_dhdr, doubl
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(grad_out, 0, 4 * sizeof(double), st);
     if (e != cudaSuccess) return err_cuda(e, "gradient reset");
-    // the LUT error word of the backward's replays: the forward already reported any overflow
     e = ktd::launch_diff_backward(d->sc_rec, d->cam_rec, d->camd_rec, d->dcamd_rec, record_of(d), d->dl_rec,
-                                  reinterpret_cast<const float4*>(dl_dhdr), grad_out, d->ctl + 2, st);
+                                  reinterpret_cast<const float4*>(dl_dhdr), grad_out, d->work, st);
     if (e != cudaSuccess) return err_cuda(e, "diff backward launch");
     return KT_OK;
 }
@@ -420,7 +426,7 @@ kt_status kt_diff_get_info(kt_diff* d, kt_diff_info* info) {
     info->segments_capacity = d->cap;
     info->overflow_rays = h[1];
     info->record_bytes = (uint64_t)info->segments_used * d->seg_bytes + (uint64_t)d->n_px * sizeof(ktd::DiffRay);
-    info->device_bytes = (uint64_t)d->cap * d->seg_bytes + (uint64_t)d->n_px * sizeof(ktd::DiffRay) +
+    info->device_bytes = (uint64_t)d->cap * d->seg_bytes + (uint64_t)d->n_px * (sizeof(ktd::DiffRay) + 8) +
                          (uint64_t)d->cfg.lut_size * (sizeof(float4) + 2 * (sizeof(float) + 3 * sizeof(double))) +
                          4 * sizeof(unsigned);
     return KT_OK;
