@@ -88,6 +88,9 @@ def olib() -> C.CDLL:
         L.kto_dense_slope.restype = C.c_double
         L.kto_crossing_root.argtypes = [C.c_void_p, C.c_double]
         L.kto_crossing_root.restype = C.c_double
+        L.kto_diff_render.argtypes = [C.POINTER(KtoScene), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int]
+        L.kto_diff_render.restype = C.c_int
         L.kto_fbm.argtypes = [C.c_double, C.c_double, C.c_int, C.c_uint32]
         L.kto_fbm.restype = C.c_double
         L.kto_aces.argtypes = [C.c_double]
@@ -255,3 +258,24 @@ class RefKernel:
         if self.tex is not None:
             self.L.ktref_free_textures(C.byref(self.tex))
             self.tex = None
+
+
+def diff_render(cfg, view, theta, pixels=None, threads: int = 0):
+    """Forward-mode f64 reference of the differentiable trace (stated physics, spp 1, no noise):
+    returns (colour [n,3], d colour / d theta [n,3,4], info [n,3] = term, hits, steps) for the
+    flat pixel indices `pixels` (all pixels when None).  view: the product's KtDiffView;
+    theta = (spin, inclination deg, temperature scale, disk outer radius)."""
+    from kerrtrace_b200 import KtCamera
+    sc = Scene(cfg, KtCamera(), mode=1, tex_mode=0)
+    n = cfg.width * cfg.height if pixels is None else len(pixels)
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    v = np.array([view.observer_r, view.azimuth_deg, view.fov_deg, view.base_temperature_scale], np.float64)
+    th = np.ascontiguousarray(theta, np.float64)
+    col = np.zeros((n, 3))
+    dcol = np.zeros((n, 3, 4))
+    info = np.zeros((n, 3), np.int32)
+    rc = olib().kto_diff_render(C.byref(sc.s), v.ctypes.data, th.ctypes.data, None if pix is None else pix.ctypes.data,
+                                n, col.ctypes.data, dcol.ctypes.data, info.ctypes.data, threads)
+    if rc != 0:
+        raise ValueError(f"oracle diff render failed ({rc})")
+    return col, dcol, info

@@ -569,6 +569,311 @@ RayResult trace_ray(const kto_scene& s, const Derived& dv, const float dirf[3], 
     return out;
 }
 
+// ---- forward-mode derivatives of the stated-physics image ---------------------------------
+// The reference gradient of the differentiable trace: the f64 stated-physics trace (mode 1,
+// spp 1 at pixel centres, no noise, exact LUT weights) carried on D4 numbers, a value and its
+// derivatives in theta = (spin, inclination in degrees, temperature scale, disk outer radius).
+// Step sizes and every discrete decision (acceptance, crossings, disk membership, termination)
+// are taken on the values, so the derivative is that of the frozen-step model.  The crossing
+// root is differentiated by the implicit-function theorem.
+struct D4 {
+    double v, d[4];
+    D4(double x = 0.0) : v(x), d{0.0, 0.0, 0.0, 0.0} {}
+    static D4 seed(double x, int k) {
+        D4 r(x);
+        r.d[k] = 1.0;
+        return r;
+    }
+};
+D4 operator+(const D4& a, const D4& b) {
+    D4 r(a.v + b.v);
+    for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+D4 operator-(const D4& a, const D4& b) {
+    D4 r(a.v - b.v);
+    for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+D4 operator-(const D4& a) {
+    D4 r(-a.v);
+    for (int i = 0; i < 4; ++i) r.d[i] = -a.d[i];
+    return r;
+}
+D4 operator*(const D4& a, const D4& b) {
+    D4 r(a.v * b.v);
+    for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+D4 operator/(const D4& a, const D4& b) {
+    D4 r(a.v / b.v);
+    for (int i = 0; i < 4; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
+    return r;
+}
+D4& operator+=(D4& a, const D4& b) { return a = a + b; }
+D4& operator*=(D4& a, const D4& b) { return a = a * b; }
+D4 d4_chain(const D4& x, double f, double df) {
+    D4 r(f);
+    for (int i = 0; i < 4; ++i) r.d[i] = df * x.d[i];
+    return r;
+}
+D4 d4_sqrt(const D4& x) { const double q = std::sqrt(x.v); return d4_chain(x, q, q > 0 ? 0.5 / q : 0.0); }
+D4 d4_cbrt(const D4& x) { const double q = std::cbrt(x.v); return d4_chain(x, q, q != 0 ? 1.0 / (3.0 * q * q) : 0.0); }
+D4 d4_exp(const D4& x) { const double q = std::exp(x.v); return d4_chain(x, q, q); }
+D4 d4_log(const D4& x) { return d4_chain(x, std::log(x.v), 1.0 / x.v); }
+D4 d4_sin(const D4& x) { return d4_chain(x, std::sin(x.v), std::cos(x.v)); }
+D4 d4_cos(const D4& x) { return d4_chain(x, std::cos(x.v), -std::sin(x.v)); }
+D4 d4_acos(const D4& x) { return d4_chain(x, std::acos(x.v), -1.0 / std::sqrt(1.0 - x.v * x.v)); }
+
+template <> struct M<D4> {
+    static D4 sqrt_(const D4& x) { return d4_sqrt(x); }
+};
+
+// ISCO and Page-Thorne flux factor (isco / nt_factor above) on D4
+D4 isco_d4(const D4& an) {
+    const D4 z1 = D4(1.0) + d4_cbrt(D4(1.0) - an * an) * (d4_cbrt(D4(1.0) + an) + d4_cbrt(D4(1.0) - an));
+    const D4 z2 = d4_sqrt(D4(3.0) * an * an + z1 * z1);
+    D4 inside = (D4(3.0) - z1) * (D4(3.0) + z1 + D4(2.0) * z2);
+    if (inside.v < 0.0) inside = D4(0.0);
+    return D4(3.0) + z2 - d4_sqrt(inside);
+}
+D4 nt_factor_d4(const D4& r, const D4& an, const D4& r_isco, double inv_m) {
+    if (!(r.v > r_isco.v)) return D4(0.0);
+    const D4 rn = r * inv_m, rin = r_isco * inv_m;
+    const D4 x = d4_sqrt(rn), xms = d4_sqrt(rin);
+    const D4 base = d4_acos(-an) * (1.0 / 3.0);
+    const double step = 2.0943951023931957;
+    const D4 roots[3] = {D4(2.0) * d4_cos(base), D4(2.0) * d4_cos(base - D4(step)), D4(2.0) * d4_cos(base + D4(step))};
+    D4 sum(0.0);
+    for (int i = 0; i < 3; ++i) {
+        const D4 xi = roots[i];
+        const D4 den = xi * (xi - roots[(i + 1) % 3]) * (xi - roots[(i + 2) % 3]);
+        if (!(den.v > 0.0)) continue;
+        const D4 coef = D4(3.0) * (xi - an) * (xi - an) / den;
+        const D4 val = (x - xi) / (xms - xi);
+        if (val.v > 0.0) sum += coef * d4_log(val);
+    }
+    const D4 q = x - xms - D4(1.5) * an * d4_log(x / xms) - sum;
+    const D4 geo = rn * (rn * x - D4(3.0) * x + D4(2.0) * an);
+    const D4 f = q / geo;
+    return f.v > 0.0 ? f : D4(0.0);
+}
+
+D4 dense_d4(const D4& y0, const D4& y1, const D4& k1, const D4& k3, const D4& k4, const D4& k5, const D4& k6,
+            const D4& k7, double h, const D4& t) {
+    using C = Tab<double>;
+    const D4 q2 = y1 - y0, q3 = y0 + h * k1 - y1, q4 = D4(2.0) * (y1 - y0) - h * (k1 + k7);
+    const D4 q5 = h * (C::d1 * k1 + C::d3 * k3 + C::d4 * k4 + C::d5 * k5 + C::d6 * k6 + C::d7 * k7);
+    const D4 t2 = t * t;
+    return y0 + t * (q2 + q3) - t2 * (q3 - q4 - q5) - t2 * t * (q4 + D4(2.0) * q5) + t2 * t2 * q5;
+}
+
+// Inputs of the differentiable trace that depend on theta, shared by all pixels.
+struct DiffSetup {
+    D4 a, aa, r_in, r_out, ts;
+    D4 pos[3], fwd[3], rgt[3], up[3];
+    double fov, Mm;
+    std::vector<D4> lut;
+};
+
+struct DiffRay {
+    D4 col[3];
+    int32_t term, hits, steps;
+};
+
+DiffRay trace_ray_diff(const kto_scene& s, const Derived& dv, const DiffSetup& ds, uint32_t px, uint32_t py) {
+    using C = Tab<double>;
+    DiffRay out;
+    out.term = 0;
+    out.hits = 0;
+    out.steps = 0;
+    for (int c = 0; c < 3; ++c) out.col[c] = D4(0.0);
+    const D4 a = ds.a, aa = ds.aa;
+    const double Mm = ds.Mm;
+    const double W = (double)s.width, H = (double)s.height;
+    const double u = ((px + 0.5) * (2.0 / W) - 1.0) * (W / H) * ds.fov;
+    const double v = (1.0 - (py + 0.5) * (2.0 / H)) * ds.fov;
+    D4 dir[3];
+    for (int c = 0; c < 3; ++c) dir[c] = u * ds.rgt[c] + v * ds.up[c] + ds.fwd[c];
+    // null initialisation (as trace_ray)
+    const D4 dl = d4_sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    const D4 n[3] = {dir[0] / dl, dir[1] / dl, dir[2] / dl};
+    D4 st[6] = {ds.pos[0], ds.pos[1], ds.pos[2], D4(0.0), D4(0.0), D4(0.0)};
+    const D4 x = st[0], y = st[1], z = st[2];
+    const D4 r0 = ks_radius<D4>(x, y, z, aa);
+    const D4 r2 = r0 * r0;
+    const D4 Dd = r2 + aa;
+    const D4 l[3] = {(r0 * x - a * z) / Dd, y / r0, (r0 * z + a * x) / Dd};
+    const D4 Hk = D4(Mm) * r2 * r0 / (r2 * r2 + aa * y * y);
+    const D4 ln = l[0] * n[0] + l[1] * n[1] + l[2] * n[2];
+    const D4 gtt = D4(-1.0) + D4(2.0) * Hk, gtn = D4(2.0) * Hk * ln, gnn = D4(1.0) + D4(2.0) * Hk * ln * ln;
+    const D4 kt = (-gtn - d4_sqrt(gtn * gtn - gtt * gnn)) / gtt;
+    const D4 pt = gtt * kt + gtn;
+    for (int c = 0; c < 3; ++c) st[3 + c] = n[c] + D4(2.0) * Hk * l[c] * (kt + ln);
+    double h = dv.h0;
+    D4 tau(1.0);
+    D4 k1[6];
+    bool have_fsal = false;
+    const double hor = (double)dv.rh + dv.hor_eps;
+    const int nl = (int)s.lut_size;
+    for (uint32_t i = 0; i < s.max_steps && tau.v > dv.cutoff; ++i) {
+        const double rc = ks_radius<double>(st[0].v, st[1].v, st[2].v, aa.v);
+        const double Hc = Mm * rc * rc * rc / (rc * rc * rc * rc + aa.v * st[1].v * st[1].v);
+        double tt = (Hc - 0.05) / (0.3 - 0.05);
+        tt = std::min(std::max(tt, 0.0), 1.0);
+        const double tol = dv.tol * (5.0 - 4.0 * tt);
+        D4 k[7][6], nx[6], yy[6];
+        double hs = h;
+        bool accepted = false, k1_ready = have_fsal;
+        uint32_t att = 0;
+        if (have_fsal) for (int c = 0; c < 6; ++c) k[0][c] = k1[c];
+        while (!accepted && att < s.max_attempts) {
+            hs = h;
+            if (!k1_ready) {
+                hamilton_rhs<D4>(st, pt, a, aa, D4(Mm), k[0], true);
+                k1_ready = true;
+            }
+            static const double A[6][5] = {{C::a21, 0, 0, 0, 0},
+                                           {C::a31, C::a32, 0, 0, 0},
+                                           {C::a41, C::a42, C::a43, 0, 0},
+                                           {C::a51, C::a52, C::a53, C::a54, 0},
+                                           {C::a61, C::a62, C::a63, C::a64, C::a65},
+                                           {C::b1, 0, C::b3, C::b4, C::b5}};
+            for (int j = 1; j < 6; ++j) {
+                for (int c = 0; c < 6; ++c) {
+                    D4 acc(0.0);
+                    for (int q = 0; q < j; ++q) acc += A[j - 1][q] * k[q][c];
+                    yy[c] = st[c] + hs * acc;
+                }
+                hamilton_rhs<D4>(yy, pt, a, aa, D4(Mm), k[j], true);
+            }
+            for (int c = 0; c < 6; ++c)
+                nx[c] = st[c] + hs * (C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] + C::b6 * k[5][c]);
+            hamilton_rhs<D4>(nx, pt, a, aa, D4(Mm), k[6], true);
+            bool all_nan = true;
+            double emax = -std::numeric_limits<double>::infinity();
+            for (int c = 0; c < 6; ++c) {
+                const double e = hs * ((C::b1 - C::bh1) * k[0][c].v + (C::b3 - C::bh3) * k[2][c].v +
+                                       (C::b4 - C::bh4) * k[3][c].v + (C::b5 - C::bh5) * k[4][c].v +
+                                       (C::b6 - C::bh6) * k[5][c].v - C::bh7 * k[6][c].v);
+                const double ec = std::fabs(e) / (tol * std::max(std::fabs(st[c].v), 1.0));
+                if (!std::isnan(ec)) {
+                    all_nan = false;
+                    emax = std::max(emax, ec);
+                }
+            }
+            const double errv = all_nan ? std::numeric_limits<double>::quiet_NaN() : emax;
+            if (errv <= 1.0) accepted = true;
+            h = hs * 0.9 * std::pow(errv, -0.2);
+            att++;
+        }
+        D4 prev[6];
+        for (int c = 0; c < 6; ++c) {
+            prev[c] = st[c];
+            st[c] = nx[c];
+        }
+        out.steps++;
+        if (accepted) {
+            for (int c = 0; c < 6; ++c) k1[c] = k[6][c];
+            have_fsal = true;
+        } else {
+            have_fsal = false;
+        }
+        if (std::isnan(st[1].v)) {
+            out.term = 3;
+            break;
+        }
+        const double r_now = ks_radius<double>(st[0].v, st[1].v, st[2].v, aa.v);
+        if (r_now < hor) {
+            out.term = 1;
+            break;
+        }
+        if ((prev[1].v < 0 && st[1].v >= 0) || (prev[1].v > 0 && st[1].v <= 0)) {
+            const double y0 = prev[1].v, y1 = st[1].v;
+            double tv = (y0 - y1) != 0.0 ? y0 / (y0 - y1) : 0.5;
+            tv = std::min(std::max(tv, 0.0), 1.0);
+            tv = crossing_root<double>(y0, y1, k[0][1].v, k[2][1].v, k[3][1].v, k[4][1].v, k[5][1].v, k[6][1].v, hs, tv);
+            // y(t*) = 0 on the dense output: dt* = -dy / y'(t*)
+            const D4 yc = dense_d4(prev[1], st[1], k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], hs, D4(tv));
+            const double slope = dense_slope<double>(y0, y1, k[0][1].v, k[2][1].v, k[3][1].v, k[4][1].v, k[5][1].v,
+                                                     k[6][1].v, hs, tv);
+            D4 t(tv);
+            if (slope != 0.0)
+                for (int q = 0; q < 4; ++q) t.d[q] = -yc.d[q] / slope;
+            D4 hp[6];
+            for (int c = 0; c < 6; ++c)
+                hp[c] = dense_d4(prev[c], st[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c], hs, t);
+            const D4 xh = hp[0], zh = hp[2];
+            const D4 rhit = ks_radius<D4>(xh, D4(0.0), zh, aa);
+            if (rhit.v >= ds.r_in.v && rhit.v <= ds.r_out.v) {
+                const double sqM = std::sqrt(Mm);
+                const D4 rs = d4_sqrt(rhit);
+                const D4 disc = D4(1.0) - D4(3.0 * Mm) / rhit + D4(2.0 * sqM) * a / (rhit * rs);
+                if (disc.v > 0) {
+                    const D4 omega = -D4(sqM) / (rhit * rs + a * sqM);
+                    const D4 D2 = rhit * rhit + aa;
+                    const D4 lx = (rhit * xh - a * zh) / D2, lz = (rhit * zh + a * xh) / D2;
+                    const D4 ldotp = lx * hp[3] + lz * hp[5];
+                    const D4 ldotxi = lx * zh - lz * xh;
+                    const D4 Hh = D4(Mm) / rhit;
+                    const D4 L = (zh * hp[3] - xh * hp[5]) + D4(2.0) * Hh * ldotxi * (ldotp + kt);
+                    const D4 g = D4(1.0) / ((D4(1.0) / d4_sqrt(disc)) * (D4(1.0) - omega * (L / (-pt))));
+                    const D4 span = ds.r_out - ds.r_in;
+                    const D4 uu = span.v > 0 ? (rhit - ds.r_in) / span : D4(0.0);
+                    // texture-style coordinate of the LUT fetch, exact weight
+                    const D4 xl = uu * (double)nl - 0.5;
+                    const double fl = std::floor(xl.v);
+                    int i0 = (int)std::min(std::max(fl, -1.0), (double)(nl - 1));
+                    int i1 = i0 + 1;
+                    i0 = std::max(i0, 0);
+                    i1 = std::min(i1, nl - 1);
+                    const D4 wl = xl - fl;
+                    const D4 sampled = ds.lut[i0] + wl * (ds.lut[i1] - ds.lut[i0]);
+                    const D4 Tm = ds.ts * sampled * g;
+                    if (std::isfinite(Tm.v) && Tm.v > 0) {
+                        out.hits++;
+                        D4 c3[3] = {D4(0.0), D4(0.0), D4(0.0)};
+                        if (Tm.v <= (double)s.lut_max_temp) {
+                            const D4 pos = Tm / (double)s.lut_max_temp * (double)(nl - 1);
+                            const double fb = std::floor(pos.v);
+                            int j0 = (int)std::min(std::max(fb, -1.0), (double)(nl - 1));
+                            int j1 = j0 + 1;
+                            j0 = std::max(j0, 0);
+                            j1 = std::min(j1, nl - 1);
+                            const D4 wb = pos - fb;
+                            for (int c = 0; c < 3; ++c) {
+                                const double e0 = s.bb_lut[4 * j0 + c], e1 = s.bb_lut[4 * j1 + c];
+                                c3[c] = D4(e0) + wb * (e1 - e0);
+                            }
+                        }
+                        const D4 luma = 0.2126 * c3[0] + 0.7152 * c3[1] + 0.0722 * c3[2];
+                        const D4 ls = luma / dv.wl_step;
+                        const D4 alpha = D4(1.0) - d4_exp(-ls * 0.5);
+                        for (int c = 0; c < 3; ++c) out.col[c] += c3[c] * alpha * tau;
+                        tau *= D4(1.0) - alpha;
+                    }
+                }
+            }
+        }
+        if (r_now > dv.escape) {
+            double ke[6], stv[6];
+            for (int c = 0; c < 6; ++c) stv[c] = st[c].v;
+            hamilton_rhs<double>(stv, pt.v, a.v, aa.v, Mm, ke, true);
+            const double nrm = std::sqrt(ke[0] * ke[0] + ke[1] * ke[1] + ke[2] * ke[2]);
+            const double ex = ke[0] / nrm, ey = ke[1] / nrm, ez = ke[2] / nrm;
+            const double lon = std::atan2(ez, ex), lat = std::asin(ey);
+            const double gs = (double)dv.sky_spacing, th = (double)(float)dv.thick;
+            const double dlon = std::fmod(std::fabs(lon), gs), dlat = std::fmod(std::fabs(lat), gs);
+            const bool grid = (dlon < th || dlon > gs - th) || (dlat < th || dlat > gs - th) || (std::fabs(lat) < th * 3.0);
+            if (grid)
+                for (int c = 0; c < 3; ++c) out.col[c] += dv.sky_int * tau;
+            out.term = 2;
+            break;
+        }
+    }
+    return out;
+}
+
 void pixel_dir(const kto_scene& s, const Derived& dv, uint32_t px, uint32_t py, uint32_t smp, float dir[3]) {
     float jx, jy;
     if (s.mode == 1 && s.spp == 1) {
@@ -788,6 +1093,71 @@ void kto_rhs_reference(const double* st, double pt, double a, double mass, doubl
 }
 double kto_dense(const double* q, double t) { return dense<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t); }
 double kto_dense_slope(const double* q, double t) { return dense_slope<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t); }
+// Differentiable trace (forward mode), stated physics, spp 1, no noise: colour (3 per pixel,
+// final scale applied) and its derivatives in theta (3 x 4 per pixel, row = channel), plus
+// (term, hits, steps) per pixel.  view = (observer r, azimuth deg, fov deg, base temperature
+// scale); theta = (spin, inclination deg, temperature scale, disk outer radius).  The scene's
+// spin, disk_outer_radius and disk_temperature_scale are replaced by theta.
+int kto_diff_render(const kto_scene* sp, const double* view, const double* theta, const uint32_t* pixels,
+                    int64_t n_pixels, double* color, double* dcolor, int32_t* info, int threads) {
+    if (!sp || !view || !theta || !color || !dcolor) return -1;
+    kto_scene s = *sp;
+    if (s.mode != 1 || s.spp != 1 || s.noise_enabled) return -2;
+    s.spin = (float)theta[0];
+    s.disk_outer_radius = (float)theta[3];
+    s.disk_temperature_scale = (float)(view[3] * theta[2]);
+    Derived dv;
+    if (!derive(s, &dv)) return -3;
+    DiffSetup ds;
+    const double inv_m = 1.0 / (double)s.mass;
+    ds.Mm = (double)s.mass;
+    ds.a = D4::seed(theta[0], 0);
+    ds.aa = ds.a * ds.a;
+    const D4 an = ds.a * inv_m;
+    ds.r_in = isco_d4(an) * (double)s.mass;
+    ds.r_out = D4::seed(theta[3], 3);
+    D4 sc = D4::seed(theta[2], 2);
+    ds.ts = sc * view[3];
+    const int nl = (int)s.lut_size;
+    ds.lut.resize(nl);
+    for (int i = 0; i < nl; ++i) {
+        const double ratio = (double)i / (double)(nl - 1);
+        const D4 r = ds.r_in + ratio * (ds.r_out - ds.r_in);
+        const D4 f = nt_factor_d4(r, an, ds.r_in, inv_m);
+        ds.lut[i] = f.v > 0.0 ? d4_sqrt(d4_sqrt(f)) : D4(0.0);
+    }
+    const double d2r = 3.14159265358979323846 / 180.0;
+    const D4 inc = D4::seed(theta[1], 1) * d2r;
+    const double az = view[1] * d2r, r = view[0];
+    ds.pos[0] = r * d4_sin(inc) * std::cos(az);
+    ds.pos[1] = r * d4_cos(inc);
+    ds.pos[2] = r * d4_sin(inc) * std::sin(az);
+    for (int c = 0; c < 3; ++c) ds.fwd[c] = -ds.pos[c] / r;
+    ds.rgt[0] = D4(std::sin(az));
+    ds.rgt[1] = D4(0.0);
+    ds.rgt[2] = D4(-std::cos(az));
+    ds.up[0] = ds.rgt[1] * ds.fwd[2] - ds.rgt[2] * ds.fwd[1];
+    ds.up[1] = ds.rgt[2] * ds.fwd[0] - ds.rgt[0] * ds.fwd[2];
+    ds.up[2] = ds.rgt[0] * ds.fwd[1] - ds.rgt[1] * ds.fwd[0];
+    ds.fov = std::tan(view[2] * d2r / 2.0);
+    const double fs = (double)dv.final_scale;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t i = 0; i < n_pixels; ++i) {
+        const uint32_t p = pixels ? pixels[i] : (uint32_t)i;
+        const DiffRay rr = trace_ray_diff(s, dv, ds, p % s.width, p / s.width);
+        for (int c = 0; c < 3; ++c) {
+            color[3 * i + c] = rr.col[c].v * fs;
+            for (int q = 0; q < 4; ++q) dcolor[12 * i + 4 * c + q] = rr.col[c].d[q] * fs;
+        }
+        if (info) {
+            info[3 * i] = rr.term;
+            info[3 * i + 1] = rr.hits;
+            info[3 * i + 2] = rr.steps;
+        }
+    }
+    return 0;
+}
+
 double kto_crossing_root(const double* q, double t0) {
     return crossing_root<double>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], t0);
 }

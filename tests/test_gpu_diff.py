@@ -142,3 +142,32 @@ def test_fp32_adjoint_tracks_fp64(cuda):
     for j in range(3):
         assert abs(g[kt.PREC_FP32][j] - g[kt.PREC_FP64][j]) <= 2e-3 * abs(g[kt.PREC_FP64][j]), NAMES[j]
     assert abs(g[kt.PREC_FP32][3] - g[kt.PREC_FP64][3]) <= 5e-2 * abs(g[kt.PREC_FP64][3])
+
+
+def test_fp64_adjoint_matches_oracle_reference_gradient(cuda):
+    """The FP64 adjoint against the f64 CPU reference gradient (the oracle's forward-mode
+    restatement of the same frozen-step trace), on the pixels whose images agree to 1e-6 (the
+    others took a different step sequence)."""
+    import oracle
+    size = 48
+    n = size * size
+    cfg, view = workloads.c5(size, kt.PREC_FP64)
+    d = kt.Diff(cfg, view)
+    hdr = cuda.zeros((n, 4), device="cuda")
+    err = cuda.zeros(2, dtype=cuda.int32, device="cuda")
+    d.forward(THETA, hdr.data_ptr(), err.data_ptr())
+    cuda.cuda.synchronize()
+    col, dcol, _ = oracle.diff_render(cfg, view, THETA)
+    img = hdr[:, :3].double().cpu().numpy()
+    same = np.abs(img - col).max(1) <= 1e-6 * (np.abs(col).max(1) + 1e-12)
+    assert same.mean() > 0.95
+    rng = np.random.default_rng(1)
+    w = rng.standard_normal((n, 3)) + 1.0
+    w[~same] = 0.0
+    W = cuda.zeros((n, 4), device="cuda")
+    W[:, :3] = cuda.tensor(w, dtype=cuda.float32, device="cuda")
+    g = backward(cuda, d, W)
+    ref = np.einsum("pc,pcj->j", W[:, :3].double().cpu().numpy(), dcol)
+    for j, tol in enumerate((1e-5, 1e-5, 1e-6, 1e-4)):
+        assert abs(g[j] - ref[j]) <= tol * abs(ref[j]), (NAMES[j], g[j], ref[j])
+    d.close()

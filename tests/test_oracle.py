@@ -279,3 +279,25 @@ def test_schwarzschild_capture_threshold(kt):
     escaped = term == oracle.TERM_ESCAPE
     assert np.all(captured[b < bc - 0.15]), (b[~captured & (b < bc - 0.15)])
     assert np.all(escaped[b > bc + 0.15]), (b[~escaped & (b > bc + 0.15)])
+
+
+def test_diff_reference_gradient_against_its_own_differences():
+    """The oracle's forward-mode gradient of the stated-physics image: in the temperature scale
+    and the disk outer radius (which leave the step sequence alone) it equals central
+    differences of the oracle's own trace, pixel by pixel."""
+    from kerrtrace_b200 import workloads
+    cfg, view = workloads.c5(32, 2)
+    th = np.array(workloads.C5_START)
+    col, dcol, info = oracle.diff_render(cfg, view, th)
+    assert (info[:, 1] > 0).sum() > 200
+    for j, e, tol in ((2, 1e-6, 1e-8), (3, 1e-5, 1e-4)):
+        tp, tm = th.copy(), th.copy()
+        tp[j] += e
+        tm[j] -= e
+        cp, _, ip = oracle.diff_render(cfg, view, tp)
+        cm, _, im = oracle.diff_render(cfg, view, tm)
+        same = (ip == info).all(1) & (im == info).all(1) & (col.max(1) > 0)
+        fd = (cp - cm) / (2 * e)
+        a = dcol[:, :, j]
+        rel = np.abs(a - fd)[same].max(1) / (np.abs(fd[same]).max(1) + 1e-9 * np.abs(fd).max())
+        assert np.median(rel) < tol, (j, np.median(rel))
