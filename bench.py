@@ -40,9 +40,9 @@ sys.path.insert(0, str(ROOT))
 
 
 # DRAM bytes per ray of the trace kernel from an ncu capture of the c2 scene at 960x540
-# (dram__bytes_read.sum 156928 B + dram__bytes_write.sum 0 B over 518400 rays): the HDR output
+# (dram__bytes_read.sum 149504 B + dram__bytes_write.sum 0 B over 518400 rays): the HDR output
 # stays in L2, the kernel reads only its LUTs and parameters.
-TRACE_TRAFFIC_PER_RAY = 156928 / 518400
+TRACE_TRAFFIC_PER_RAY = 149504 / 518400
 
 
 def parse():
@@ -457,7 +457,7 @@ def run_ours(args, rank, world, local):
                                f"{sms} SMs x 128 lanes x 2 flops",
                 "traffic": int(TRACE_TRAFFIC_PER_RAY * n * cfg.spp),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one trace launch "
-                                  "(c2 scene at 960x540: 156928 + 0 B), scaled to this launch by its rays",
+                                  "(c2 scene at 960x540: 149504 + 0 B), scaled to this launch by its rays",
                 "trace_ms": round(trace_ms, 4),
                 "post_ms": round(sum(t_post) / len(t_post), 4),
                 "work": {"rays": int(stats.rays), "steps": int(stats.steps), "attempts": int(stats.attempts),
