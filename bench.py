@@ -9,7 +9,9 @@ radius 24, ACES + sRGB): the trace kernel plus the post-processing kernel.
   e2e     the same metric through the public renderer API (kt_renderer_submit_render +
           ready_frame + finish_frame): per frame the camera goes host -> device as launch
           arguments and the 0x00RRGGBB frame plus its LUT error word come back into pinned
-          host memory; wall-clock per frame after a device synchronise
+          host memory; two frames in flight as the reference host keeps them (the copy of one
+          overlaps the trace of the next); wall-clock from the first submit to the last frame
+          handed back
   roofline  FP32 work of the trace kernel (counted RHS evaluations / attempts / steps x the
           static op counts in kerrtrace_b200/flops.py) / its event-timed duration, against the
           FP32 FMA peak at the SM clock sampled during the run (148 SMs x 128 lanes x 2 flops)
@@ -58,6 +60,7 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"],
                     help="arithmetic of the main loop (mixed / fp64 need --mode spec)")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--no-c3", action="store_true", help="skip the 4096^2 x 8-draw precision ablation")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -250,6 +253,106 @@ def precision_leg(cfg, cam, local, reps: int) -> dict:
     return runs
 
 
+def _log_hist(x, hist, lo: float = -12.0, bins: int = 1300):
+    """Accumulate log10 of positive relative errors into 0.01-decade bins (zeros into bin 0)."""
+    import torch
+    v = torch.log10(x.clamp_min(10.0 ** lo))
+    hist += torch.histc(v, bins=bins, min=lo, max=lo + bins / 100.0).double()
+
+
+def _hist_quantile(hist, q: float, lo: float = -12.0):
+    import torch
+    c = torch.cumsum(hist, 0)
+    if float(c[-1]) == 0:
+        return None
+    k = int(torch.searchsorted(c, q * c[-1]))
+    return float(10.0 ** (lo + (k + 1) / 100.0))
+
+
+def c3_leg(local, draws: int = 8, size: int = 4096) -> dict:
+    """Mixed-precision ablation: 8 draws of (spin, inclination) seen at 4096^2 (FOV 20, r_obs
+    60, stated physics, tolerance 1e-6), each traced in FP64, FP32 and mixed precision.  Per
+    precision: Mrays/s over all draws (event-timed trace kernel, launch shape tuned on draw 0);
+    for FP32 and mixed the per-pixel relative error against the FP64 run of HDR RGB and of the
+    radius and redshift of the first disk crossing (max, p99, p99.9 over all draws; quantiles
+    from 0.01-decade histograms), the fraction of pixels above 1e-3 and the hit/miss class
+    mismatches."""
+    import torch
+
+    import kerrtrace_b200 as kt
+    from kerrtrace_b200 import autotune, workloads
+
+    n = size * size
+    stream = torch.cuda.current_stream().cuda_stream
+    hdr = {p: torch.zeros((n, 4), device="cuda") for p in ("fp64", "fp32", "mixed")}
+    aux = {p: torch.zeros((n, 4), device="cuda") for p in ("fp64", "fp32", "mixed")}
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    precs = (("fp64", kt.PREC_FP64), ("fp32", kt.PREC_FP32), ("mixed", kt.PREC_MIXED))
+    tuning, ms_total, steps, zone = {}, {p: 0.0 for p, _ in precs}, {p: 0 for p, _ in precs}, {p: 0 for p, _ in precs}
+    acc = {p: {"hist": {k: torch.zeros(1300, dtype=torch.float64, device="cuda") for k in ("hdr", "r", "g")},
+               "max": {"hdr": 0.0, "r": 0.0, "g": 0.0}, "over": 0, "class": 0, "hits": 0} for p in ("fp32", "mixed")}
+    per_draw = []
+    for dr in range(draws):
+        cfg, cam = workloads.c3(dr, size)
+        for pname, prec in precs:
+            c = cfg.copy()
+            c.precision = prec
+            ctx = kt.Context(c, local)
+            if dr == 0:
+                tuning[pname] = autotune.autotune(ctx, cam, reps=1, stream=stream).best
+            ctx.set_tuning(**tuning[pname])
+            st = ctx.trace_counted(cam, hdr[pname].data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO,
+                                   aux[pname].data_ptr())
+            ctx.trace(cam, hdr[pname].data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.trace(cam, hdr[pname].data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+            e1.record()
+            torch.cuda.synchronize()
+            ms_total[pname] += e0.elapsed_time(e1)
+            steps[pname] += int(st.steps)
+            zone[pname] += int(st.fp64_steps)
+            ctx.close()
+        ref = hdr["fp64"][:, :3].double()
+        floor = 1e-6 * float(ref.abs().max())
+        hit_ref = torch.isfinite(aux["fp64"][:, 0])
+        row = {"spin": cfg.spin, "inclination_deg": workloads.c3_draws()[dr][1]}
+        for pname in ("fp32", "mixed"):
+            a = acc[pname]
+            rel = ((hdr[pname][:, :3].double() - ref).abs() / ref.abs().clamp_min(floor)).max(1).values
+            _log_hist(rel, a["hist"]["hdr"])
+            a["max"]["hdr"] = max(a["max"]["hdr"], float(rel.max()))
+            over = int((rel > 1e-3).sum())
+            a["over"] += over
+            hit = torch.isfinite(aux[pname][:, 0])
+            cls = int((hit != hit_ref).sum())
+            a["class"] += cls
+            both = hit & hit_ref
+            a["hits"] += int(both.sum())
+            for k, col in (("r", 0), ("g", 1)):
+                x = aux[pname][both, col].double()
+                y = aux["fp64"][both, col].double()
+                rk = (x - y).abs() / y.abs()
+                _log_hist(rk, a["hist"][k])
+                a["max"][k] = max(a["max"][k], float(rk.max()) if rk.numel() else 0.0)
+            row[pname] = {"hdr_over_1e-3": over, "class_mismatch": cls}
+        per_draw.append(row)
+    out = {"size": size, "draws": per_draw, "tuning": tuning}
+    for pname, _ in precs:
+        out[pname] = {"mrays_s": round(draws * n / ms_total[pname] / 1e3, 1), "trace_ms_per_draw": round(ms_total[pname] / draws, 3),
+                      "steps": steps[pname], "fp64_zone_steps": zone[pname]}
+    for pname in ("fp32", "mixed"):
+        a = acc[pname]
+        e = {"pixels": draws * n, "hit_pixels_compared": a["hits"], "hdr_frac_over_1e-3": a["over"] / (draws * n),
+             "hit_class_mismatch": a["class"]}
+        for k, name in (("hdr", "hdr"), ("r", "r_cross"), ("g", "g")):
+            e[f"{name}_max"] = a["max"][k]
+            e[f"{name}_p99"] = _hist_quantile(a["hist"][k], 0.99)
+            e[f"{name}_p999"] = _hist_quantile(a["hist"][k], 0.999)
+        out[pname]["err_vs_fp64"] = e
+    return out
+
+
 def batch_leg(local, reps: int) -> dict:
     """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
     random spins, inclinations, observer and disk radii): one batched launch, the same launch
@@ -423,20 +526,24 @@ def run_ours(args, rank, world, local):
     rend.set_tuning(ctx.tuning())
     cam_args = (list(cam.cam_pos), list(cam.fwd), list(cam.rgt), list(cam.up), cam.fov_scale)
 
-    def frame():
-        assert rend.submit_render(*cam_args)
-        rend.wait()
-        idx, data = rend.ready_frame()
-        rend.finish_frame(idx)
-        return data
+    def frames(k):
+        """k frames the way the reference host drives CudaRenderer: submit while a frame buffer
+        is free (two in flight), poll ready_frame, hand each finished frame back."""
+        submitted = done = 0
+        while done < k:
+            if submitted < k and rend.submit_render(*cam_args):
+                submitted += 1
+                continue
+            got = rend.ready_frame()
+            if got is not None:
+                rend.finish_frame(got[0])
+                done += 1
 
-    for _ in range(args.warmup):
-        frame()
+    frames(args.warmup)
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        frame()
+    frames(args.steps)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     rend.close()
     e2e = {"value": round(rays_all / e2e_s / 1e6, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 52,
@@ -463,6 +570,9 @@ def run_ours(args, rank, world, local):
                 "work": {"rays": int(stats.rays), "steps": int(stats.steps), "attempts": int(stats.attempts),
                          "rhs_evals": int(stats.rhs_evals), "frozen_rays": int(stats.frozen_rays),
                          "flops": work}}
+    # trace (+ the pixel-ranking pass of a long-rays-first tuning) + bloom and post passes
+    bloom_on = bool(cfg.bloom_enabled) and int(math.ceil(cfg.bloom_radius)) > 0 and cfg.bloom_intensity > 0
+    launches_per_step = 1 + (1 if t.order == kt.ORDER_LONG_FIRST else 0) + (2 if bloom_on else 1)
     line = {
         "metric": "Mrays/s 1080p (c2 scene, trace + post)", "value": round(value, 3), "unit": "Mrays/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -475,12 +585,14 @@ def run_ours(args, rank, world, local):
                    else "stated physics", "precision": args.precision,
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"replica frames x{world}"},
-        "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": 2 * args.steps,
+        "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
     }
     if tuned is not None:
         line["autotune"] = tuned.summary()
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision"] = precision_leg(cfg, cam, local, max(3, args.steps))
+    if rank == 0 and world == 1 and not args.no_c3:
+        line["c3"] = c3_leg(local)
     if rank == 0 and world == 1 and not args.no_batch:
         line["batch"] = batch_leg(local, 3)
     if rank == 0 and world == 1 and not args.no_adjoint:

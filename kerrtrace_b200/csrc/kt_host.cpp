@@ -832,13 +832,19 @@ struct kt_frame {
     uint32_t* host_image = nullptr;  // pinned
     uint32_t* err = nullptr;
     uint32_t* host_err = nullptr;    // pinned, 2 words
-    cudaEvent_t ready = nullptr;
+    cudaEvent_t computed = nullptr;  // trace + post done (on the render stream)
+    cudaEvent_t ready = nullptr;     // image and error word in pinned memory (on the copy stream)
     bool has_event = false;
+    bool used = false;               // `ready` has been recorded at least once
 };
 
+// Frames render on the legacy default stream (cudarc's default_stream(), like the reference) and
+// come back to pinned memory on a non-blocking copy stream, so that with two frames in flight
+// the copy of one overlaps the trace of the next.
 struct kt_renderer {
     kt_context* ctx = nullptr;
     cudaStream_t stream = nullptr;   // the legacy default stream, like cudarc's default_stream()
+    cudaStream_t copy = nullptr;     // non-blocking device-to-host stream
     kt_frame frames[2];
     std::deque<uint32_t> pending;
     uint32_t next_frame = 0;
@@ -859,7 +865,9 @@ void destroy_renderer(kt_renderer* r) {
             cudaFreeHost(f.host_image);
             cudaFreeHost(f.host_err);
             if (f.ready) cudaEventDestroy(f.ready);
+            if (f.computed) cudaEventDestroy(f.computed);
         }
+        if (r->copy) cudaStreamDestroy(r->copy);
         destroy_ctx(r->ctx);
     }
     delete r;
@@ -880,6 +888,14 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
     }
     DeviceGuard g(device);
     const size_t px = (size_t)cfg->width * cfg->height;
+    {
+        const cudaError_t e = cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            st = cuda_fail(e, "create copy stream");
+            destroy_renderer(r);
+            return st;
+        }
+    }
     for (auto& f : r->frames) {
         cudaError_t e;
         if ((e = cudaMalloc(&f.hdr, px * 4 * sizeof(float))) != cudaSuccess ||
@@ -889,6 +905,7 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
             (e = cudaMallocHost(&f.host_image, px * sizeof(uint32_t))) != cudaSuccess ||
             (e = cudaMallocHost(&f.host_err, 2 * sizeof(uint32_t))) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&f.ready, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&f.computed, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaMemset(f.hdr, 0, px * 4 * sizeof(float))) != cudaSuccess ||
             (e = cudaMemset(f.bloom, 0, px * 4 * sizeof(float))) != cudaSuccess ||
             (e = cudaMemset(f.image, 0, px * sizeof(uint32_t))) != cudaSuccess ||
@@ -943,14 +960,19 @@ kt_status kt_renderer_submit_render(kt_renderer* r, const float cam_pos[3], cons
     cam.fov_scale = fov_scale;
     DeviceGuard g(r->ctx->device);
     const size_t px = (size_t)r->ctx->cfg.width * r->ctx->cfg.height;
+    // the buffers of this frame may still be on their way to the host from its previous use
+    if (f.used) KT_CUDA(cudaStreamWaitEvent(r->stream, f.ready, 0), "order after the previous copy");
     KT_CUDA(cudaMemsetAsync(f.err, 0, 2 * sizeof(uint32_t), r->stream), "clear LUT error flag");
     kt_status st = kt_trace(r->ctx, r->stream, &cam, r->schedule, f.hdr, f.err);
     if (st != KT_OK) return st;
-    KT_CUDA(cudaMemcpyAsync(f.host_err, f.err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream), "read LUT error flag");
     st = kt_post_fused(r->ctx, r->stream, f.hdr, f.image);
     if (st != KT_OK) return st;
-    KT_CUDA(cudaMemcpyAsync(f.host_image, f.image, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream), "copy image back");
-    KT_CUDA(cudaEventRecord(f.ready, r->stream), "record frame event");
+    KT_CUDA(cudaEventRecord(f.computed, r->stream), "record render event");
+    KT_CUDA(cudaStreamWaitEvent(r->copy, f.computed, 0), "order the copy after the render");
+    KT_CUDA(cudaMemcpyAsync(f.host_err, f.err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->copy), "read LUT error flag");
+    KT_CUDA(cudaMemcpyAsync(f.host_image, f.image, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->copy), "copy image back");
+    KT_CUDA(cudaEventRecord(f.ready, r->copy), "record frame event");
+    f.used = true;
     f.has_event = true;
     r->pending.push_back(idx);
     r->next_frame = (idx + 1) % 2;

@@ -81,3 +81,39 @@ def test_both_schedules_render_the_same_frame(cuda):
         r.finish_frame(idx)
         r.close()
     assert np.array_equal(frames[0], frames[1])
+
+
+def test_pipelined_frames_keep_their_own_camera(cuda):
+    """Two frames in flight (the copy of one overlapping the trace of the next): each frame
+    handed back is the image of the camera it was submitted with."""
+    cfg, _ = workloads.scene("t2")
+    cams = [kt.orbit_camera(40.0, 50.0 + 6.0 * k, 30.0) for k in range(6)]
+    ctx = kt.Context(cfg)
+    n = cfg.width * cfg.height
+    hdr = cuda.zeros((n, 4), device="cuda")
+    err = cuda.zeros(2, dtype=cuda.int32, device="cuda")
+    img = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    expect = []
+    for cam in cams:
+        ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), 0, kt.SCHED_PLAIN)
+        ctx.post_fused(hdr.data_ptr(), img.data_ptr())
+        cuda.cuda.synchronize()
+        expect.append(img.cpu().numpy().view(np.uint32).copy())
+    assert not np.array_equal(expect[0], expect[1])
+    r = kt.Renderer(cfg)
+    r.set_schedule(kt.SCHED_PLAIN)
+    got, submitted, t0 = [], 0, time.time()
+    while len(got) < len(cams) and time.time() - t0 < 60:
+        if submitted < len(cams):
+            c = cams[submitted]
+            if r.submit_render(list(c.cam_pos), list(c.fwd), list(c.rgt), list(c.up), c.fov_scale):
+                submitted += 1
+                continue
+        f = r.ready_frame()
+        if f is not None:
+            got.append(f[1].copy())
+            r.finish_frame(f[0])
+    r.close()
+    assert len(got) == len(cams)
+    for k in range(len(cams)):
+        assert np.array_equal(got[k], expect[k]), k
