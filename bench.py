@@ -270,13 +270,19 @@ def _hist_quantile(hist, q: float, lo: float = -12.0):
 
 
 def c3_leg(local, draws: int = 8, size: int = 4096) -> dict:
+    """The ablation at the scene's tolerance (1e-6) and at the plain method's 1e-8."""
+    return {"size": size, "runs": [c3_run(local, tol, draws, size) for tol in (1e-6, 1e-8)]}
+
+
+def c3_run(local, tol: float, draws: int = 8, size: int = 4096) -> dict:
     """Mixed-precision ablation: 8 draws of (spin, inclination) seen at 4096^2 (FOV 20, r_obs
-    60, stated physics, tolerance 1e-6), each traced in FP64, FP32 and mixed precision.  Per
-    precision: Mrays/s over all draws (event-timed trace kernel, launch shape tuned on draw 0);
-    for FP32 and mixed the per-pixel relative error against the FP64 run of HDR RGB and of the
-    radius and redshift of the first disk crossing (max, p99, p99.9 over all draws; quantiles
-    from 0.01-decade histograms), the fraction of pixels above 1e-3 and the hit/miss class
-    mismatches."""
+    60, stated physics, tolerance `tol`), each traced in FP64, FP32, mixed precision (FP64 state
+    update inside 1.5 x the photon-orbit radius) and mixed with the FP64 update on the whole path
+    (`photon_zone_factor` 1000).  Per variant: Mrays/s over all draws (event-timed trace kernel,
+    launch shape tuned on draw 0); for the others the per-pixel relative error against the FP64
+    run of HDR RGB and of the radius and redshift of the first disk crossing (max, p99, p99.9
+    over all draws; quantiles from 0.01-decade histograms), the fraction of pixels above 1e-3
+    and the hit/miss class mismatches."""
     import torch
 
     import kerrtrace_b200 as kt
@@ -284,19 +290,23 @@ def c3_leg(local, draws: int = 8, size: int = 4096) -> dict:
 
     n = size * size
     stream = torch.cuda.current_stream().cuda_stream
-    hdr = {p: torch.zeros((n, 4), device="cuda") for p in ("fp64", "fp32", "mixed")}
-    aux = {p: torch.zeros((n, 4), device="cuda") for p in ("fp64", "fp32", "mixed")}
+    precs = (("fp64", kt.PREC_FP64, 1.5), ("fp32", kt.PREC_FP32, 1.5), ("mixed", kt.PREC_MIXED, 1.5),
+             ("mixed_whole_path", kt.PREC_MIXED, 1000.0))
+    names = [p for p, _, _ in precs]
+    hdr = {p: torch.zeros((n, 4), device="cuda") for p in names}
+    aux = {p: torch.zeros((n, 4), device="cuda") for p in names}
     err = torch.zeros(2, dtype=torch.int32, device="cuda")
-    precs = (("fp64", kt.PREC_FP64), ("fp32", kt.PREC_FP32), ("mixed", kt.PREC_MIXED))
-    tuning, ms_total, steps, zone = {}, {p: 0.0 for p, _ in precs}, {p: 0 for p, _ in precs}, {p: 0 for p, _ in precs}
+    tuning, ms_total, steps, zone = {}, {p: 0.0 for p in names}, {p: 0 for p in names}, {p: 0 for p in names}
     acc = {p: {"hist": {k: torch.zeros(1300, dtype=torch.float64, device="cuda") for k in ("hdr", "r", "g")},
-               "max": {"hdr": 0.0, "r": 0.0, "g": 0.0}, "over": 0, "class": 0, "hits": 0} for p in ("fp32", "mixed")}
+               "max": {"hdr": 0.0, "r": 0.0, "g": 0.0}, "over": 0, "class": 0, "hits": 0} for p in names[1:]}
     per_draw = []
     for dr in range(draws):
         cfg, cam = workloads.c3(dr, size)
-        for pname, prec in precs:
+        cfg.tolerance = tol
+        for pname, prec, zf in precs:
             c = cfg.copy()
             c.precision = prec
+            c.photon_zone_factor = zf
             ctx = kt.Context(c, local)
             if dr == 0:
                 tuning[pname] = autotune.autotune(ctx, cam, reps=1, stream=stream).best
@@ -317,7 +327,7 @@ def c3_leg(local, draws: int = 8, size: int = 4096) -> dict:
         floor = 1e-6 * float(ref.abs().max())
         hit_ref = torch.isfinite(aux["fp64"][:, 0])
         row = {"spin": cfg.spin, "inclination_deg": workloads.c3_draws()[dr][1]}
-        for pname in ("fp32", "mixed"):
+        for pname in names[1:]:
             a = acc[pname]
             rel = ((hdr[pname][:, :3].double() - ref).abs() / ref.abs().clamp_min(floor)).max(1).values
             _log_hist(rel, a["hist"]["hdr"])
@@ -337,11 +347,11 @@ def c3_leg(local, draws: int = 8, size: int = 4096) -> dict:
                 a["max"][k] = max(a["max"][k], float(rk.max()) if rk.numel() else 0.0)
             row[pname] = {"hdr_over_1e-3": over, "class_mismatch": cls}
         per_draw.append(row)
-    out = {"size": size, "draws": per_draw, "tuning": tuning}
-    for pname, _ in precs:
+    out = {"tolerance": tol, "draws": per_draw, "tuning": tuning}
+    for pname in names:
         out[pname] = {"mrays_s": round(draws * n / ms_total[pname] / 1e3, 1), "trace_ms_per_draw": round(ms_total[pname] / draws, 3),
                       "steps": steps[pname], "fp64_zone_steps": zone[pname]}
-    for pname in ("fp32", "mixed"):
+    for pname in names[1:]:
         a = acc[pname]
         e = {"pixels": draws * n, "hit_pixels_compared": a["hits"], "hdr_frac_over_1e-3": a["over"] / (draws * n),
              "hit_class_mismatch": a["class"]}
