@@ -276,9 +276,10 @@ def c3_leg(local, draws: int = 8, size: int = 4096) -> dict:
 
 def c3_run(local, tol: float, draws: int = 8, size: int = 4096) -> dict:
     """Mixed-precision ablation: 8 draws of (spin, inclination) seen at 4096^2 (FOV 20, r_obs
-    60, stated physics, tolerance `tol`), each traced in FP64, FP32, mixed precision (FP64 state
-    update inside 1.5 x the photon-orbit radius) and mixed with the FP64 update on the whole path
-    (`photon_zone_factor` 1000).  Per variant: Mrays/s over all draws (event-timed trace kernel,
+    60, stated physics, tolerance `tol`), each traced in FP64, FP32, mixed precision (compensated
+    FP32 update, FP64 update inside 1.5 x the photon-orbit radius), mixed without the FP64 zone
+    (`photon_zone_factor` 0.01, inside the horizon) and mixed with the FP64 update on the whole
+    path (`photon_zone_factor` 1000).  Per variant: Mrays/s over all draws (event-timed trace kernel,
     launch shape tuned on draw 0); for the others the per-pixel relative error against the FP64
     run of HDR RGB and of the radius and redshift of the first disk crossing (max, p99, p99.9
     over all draws; quantiles from 0.01-decade histograms), the fraction of pixels above 1e-3
@@ -291,7 +292,7 @@ def c3_run(local, tol: float, draws: int = 8, size: int = 4096) -> dict:
     n = size * size
     stream = torch.cuda.current_stream().cuda_stream
     precs = (("fp64", kt.PREC_FP64, 1.5), ("fp32", kt.PREC_FP32, 1.5), ("mixed", kt.PREC_MIXED, 1.5),
-             ("mixed_whole_path", kt.PREC_MIXED, 1000.0))
+             ("mixed_no_zone", kt.PREC_MIXED, 0.01), ("mixed_whole_path", kt.PREC_MIXED, 1000.0))
     names = [p for p, _, _ in precs]
     hdr = {p: torch.zeros((n, 4), device="cuda") for p in names}
     aux = {p: torch.zeros((n, 4), device="cuda") for p in names}

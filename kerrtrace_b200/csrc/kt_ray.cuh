@@ -421,12 +421,14 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
 
 // =========================================================================================
 // Mixed precision (stated physics only).  The state is a float pair: hi carries every FP32
-// computation (right-hand sides, stages, tests), lo the part of an FP64 value below hi.
-// Outside the photon zone (Kerr-Schild radius of the step start >= sc.zone_r, 1.5 x the
-// retrograde photon-orbit radius, which contains the horizon) lo is 0 and the step is exactly
-// the FP32 step.  Inside it the state update x + h sum b_i k_i runs in FP64 on hi + lo, every
-// kRenormEvery-th accepted step renormalises p onto the null cone in FP64, and the result is
-// split back into hi and lo.  The embedded error norm runs in FP64 when the tolerance is below
+// computation (right-hand sides, stages, tests), lo the rounding error of hi.  Outside the
+// photon zone (Kerr-Schild radius of the step start >= sc.zone_r, 1.5 x the retrograde
+// photon-orbit radius, which contains the horizon) the state update x + h sum b_i k_i is a
+// compensated FP32 sum: Knuth's TwoSum of hi and the increment (plus the carried lo) gives the
+// new hi and its exact rounding error, so the rounding of the update, which at tight
+// tolerances is the floor of an FP32 trace that starts far out, does not accumulate.  Inside
+// the zone the update runs in FP64 on hi + lo, every kRenormEvery-th accepted step renormalises
+// p onto the null cone in FP64, and the result is split back into hi and lo.  The embedded error norm runs in FP64 when the tolerance is below
 // 3e-7 (sc.zone_err64): the FP32 stage sum carries an absolute error of about
 // 6e-9 h |k|, under 1% of the tolerance scale above that.  A crossing is located in FP32, its
 // root refined by FP64 Newton steps on the hi + lo dense output, and the hit shaded in FP32.
@@ -437,7 +439,7 @@ constexpr int kRenormEvery = 8;
 template <>
 struct RayRun<Mixed> {
     float s[6];   // hi
-    float lo[6];  // lo (0 outside the zone)
+    float lo[6];  // rounding error of hi (compensated update outside the zone, FP64 split inside)
     float k1[6];
     double pt, kt;
     float h, tol;
@@ -558,16 +560,7 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
     const float pt = (float)ry.pt;
     if (ry.attempt == 0) {
         ry.tol = step_tolerance<float, 1>(ry.s, sc);
-        const bool zone = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa) < sc.zone_r;
-        if (!zone && ry.zone) {  // leaving the zone: fold lo into hi
-#pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                ry.s[c] = (float)((double)ry.s[c] + (double)ry.lo[c]);
-                ry.lo[c] = 0.0f;
-            }
-            ry.have_k1 = false;
-        }
-        ry.zone = zone;
+        ry.zone = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa) < sc.zone_r;
     }
     if (!ry.have_k1) {
         hamilton_rhs<float, EXACT>(ry.s, pt, a, aa, M, ry.k1);
@@ -655,8 +648,16 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
             ry.lo[c] = (float)(nd[c] - (double)ry.s[c]);
         }
     } else {
+        // TwoSum(hi, d) with d = h inc + lo: sum + e == hi + d exactly (round-to-nearest
+        // additions, written as intrinsics so that nothing contracts or reorders them)
 #pragma unroll
-        for (int c = 0; c < 6; ++c) ry.s[c] = nx[c];
+        for (int c = 0; c < 6; ++c) {
+            const float d = fmaf(h, inc[c], prev_lo[c]);
+            const float sum = __fadd_rn(prev[c], d);
+            const float bv = __fsub_rn(sum, prev[c]);
+            ry.lo[c] = __fadd_rn(__fsub_rn(prev[c], __fsub_rn(sum, bv)), __fsub_rn(d, bv));
+            ry.s[c] = sum;
+        }
     }
     ry.attempt = 0;
     if (COUNT) tl.steps++;
