@@ -191,7 +191,7 @@ template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
 
 template <class R, int MODE, bool COUNT, int MAXT>
 __global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
-    trace_plain_kernel(const Scene sc, const Camera cam,
+    trace_plain_kernel(const __grid_constant__ Scene sc, const Camera cam,
                                                            float4* __restrict__ hdr,
                                                            uint32_t* __restrict__ err,
                                                            unsigned long long* __restrict__ ctr,
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
 // divergent start-up code runs.
 template <class R, int MODE, bool COUNT, int MINB>
 __global__ void __launch_bounds__(kWavefrontBlock, MINB)
-    trace_wavefront_kernel(const Scene sc, const Camera cam, float4* __restrict__ hdr,
+    trace_wavefront_kernel(const __grid_constant__ Scene sc, const Camera cam, float4* __restrict__ hdr,
                            uint32_t* __restrict__ err, unsigned* __restrict__ queue,
                            unsigned long long* __restrict__ ctr, float4* __restrict__ aux,
                            int refill_min, const unsigned* __restrict__ order) {

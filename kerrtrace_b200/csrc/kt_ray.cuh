@@ -522,15 +522,19 @@ __device__ __forceinline__ bool ray_start_mixed(RayRun<Mixed>& ry, const Camera&
 }
 
 // Disk crossing of a mixed-precision step.  Kept out of line: it runs on few steps and would
-// otherwise raise the register count of the whole loop.  ks rows: k1, k3, k4, k5, k6, k7, lo
-// of the step start; tc: the FP32 root.  Two FP64 Newton steps on the hi + lo dense output take
-// the root to FP64 accuracy; the hit is then shaded in FP32.
-static __device__ __noinline__ void shade_mixed(RayRun<Mixed>& ry, const float* prev, const float (*ks)[6], float h,
-                                                float tc, const Scene& sc, uint32_t* err, Tally* tl) {
+// otherwise raise the register count of the whole loop.  Everything it reads or writes is
+// passed through small arrays that the caller fills only when it calls, so that the ray state
+// of the stepping loop never has its address taken (which would move it to local memory).
+// q rows: k1, k3, k4, k5, k6, k7, then hi and lo of the step start and of the step end; tc: the
+// FP32 root; ct: colour and transmittance, updated.  Two FP64 Newton steps on the hi + lo dense
+// output take the root to FP64 accuracy; the hit is then shaded in FP32.
+static __device__ __noinline__ void shade_mixed(const float (*q)[6], float h, float tc, double ptd, double ktd,
+                                                const Scene& sc, uint32_t* err, Tally* tl, float* ct) {
+    const float (*ks)[6] = q;
     double y0[6], y1[6];
     for (int c = 0; c < 6; ++c) {
-        y0[c] = (double)prev[c] + (double)ks[6][c];
-        y1[c] = (double)ry.s[c] + (double)ry.lo[c];
+        y0[c] = (double)q[6][c] + (double)q[7][c];
+        y1[c] = (double)q[8][c] + (double)q[9][c];
     }
     const double hd = (double)h;
     double t = (double)tc;
@@ -546,7 +550,7 @@ static __device__ __noinline__ void shade_mixed(RayRun<Mixed>& ry, const float* 
     for (int c = 0; c < 6; ++c)
         hit[c] = (float)dense_eval<double>(y0[c], y1[c], ks[0][c], ks[1][c], ks[2][c], ks[3][c], ks[4][c],
                                            ks[5][c], hd, t);
-    shade_hit<float, 1>(hit, (float)ry.pt, (float)ry.kt, ry.col, ry.tau, sc, err, tl);
+    shade_hit<float, 1>(hit, (float)ptd, (float)ktd, ct, ct[3], sc, err, tl);
 }
 
 template <int MODE, bool COUNT>
@@ -682,18 +686,35 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
         near_disk = rc >= sc.disk_inner * 0.999f && rc <= sc.disk_outer * 1.001f;
     }
     if (near_disk) {
-        float ks[7][6];
+        float q[10][6], ct[4];
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-            ks[0][c] = k1[c];
-            ks[1][c] = k3[c];
-            ks[2][c] = k4[c];
-            ks[3][c] = k5[c];
-            ks[4][c] = k6[c];
-            ks[5][c] = k7[c];
-            ks[6][c] = prev_lo[c];
+            q[0][c] = k1[c];
+            q[1][c] = k3[c];
+            q[2][c] = k4[c];
+            q[3][c] = k5[c];
+            q[4][c] = k6[c];
+            q[5][c] = k7[c];
+            q[6][c] = prev[c];
+            q[7][c] = prev_lo[c];
+            q[8][c] = ry.s[c];
+            q[9][c] = ry.lo[c];
         }
-        shade_mixed(ry, prev, ks, h, tc, sc, err, COUNT ? &tl : nullptr);
+        ct[0] = ry.col[0];
+        ct[1] = ry.col[1];
+        ct[2] = ry.col[2];
+        ct[3] = ry.tau;
+        if (COUNT) {
+            Tally t2 = tl;
+            shade_mixed(q, h, tc, ry.pt, ry.kt, sc, err, &t2, ct);
+            tl = t2;
+        } else {
+            shade_mixed(q, h, tc, ry.pt, ry.kt, sc, err, nullptr, ct);
+        }
+        ry.col[0] = ct[0];
+        ry.col[1] = ct[1];
+        ry.col[2] = ct[2];
+        ry.tau = ct[3];
     }
     if (ok) {
 #pragma unroll
