@@ -225,6 +225,16 @@ kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t 
 kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam,
                            int32_t schedule, float* hdr_out, uint32_t* err_word,
                            kt_trace_stats* stats, float* aux_out);
+/* Progressive sampling: the reference's per-pixel sample loop (cuda/kernel.cu:104-139) split
+ * over launches.  Traces samples [first_sample, first_sample + n_samples) of every pixel with
+ * the reference's jitter keys (pixel index << 32 | sample index), continues the running sum of
+ * the raw sample colours in accum (dev float[4*W*H]: rgb = sum, w = samples so far; read when
+ * first_sample > 0, written every call) and writes hdr_out = sum x (float)(exposure x (1.0f /
+ * samples so far)).  After samples 0..N-1, in any split, hdr_out is bit for bit the kt_trace
+ * image of the same scene at spp = N.  Samples are always jittered (also in stated physics,
+ * whose spp = 1 trace uses the pixel centre).  Plain schedule, stream-ordered. */
+kt_status kt_trace_progressive(kt_context* ctx, void* stream, const kt_camera* cam, uint32_t first_sample,
+                               uint32_t n_samples, float* accum, float* hdr_out, uint32_t* err_word);
 /* Launch shape of the trace (the autotuner's knobs, kerrtrace_b200/autotune.py).  For the
  * persistent schedule: resident blocks of 128 threads per SM (3..6; the compiler caps registers
  * per thread accordingly; only the FP32 reference-semantics kernel has the 3/5/6 variants) and
@@ -325,6 +335,33 @@ kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning);
 /* The device HDR buffer of a frame (valid until the frame is resubmitted). */
 kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev);
 void kt_renderer_destroy(kt_renderer* r);
+
+/* ---- headless mirror of the interactive loop's render policy (src/app.rs) ------------------ */
+/* A camera as the app holds it: position, yaw and pitch in degrees, vertical fov in degrees. */
+typedef struct kt_view {
+    float cam_pos[3];
+    float yaw_deg, pitch_deg, fov_deg;
+} kt_view;
+/* The app's record of the last submitted view (prev_cam_pos/yaw/pitch, prev_fov, has_frame). */
+typedef struct kt_view_state {
+    kt_view prev;
+    int32_t has_frame;
+} kt_view_state;
+/* App::new (src/app.rs:43-56): prev = the initial view, no frame yet. */
+kt_status kt_view_state_init(kt_view_state* s, const kt_view* initial);
+/* App::should_render (src/app.rs:184-198): 1 when there is no frame yet, the position moved
+ * (f32 length of the difference > 0), yaw or pitch changed by more than 1e-4, or the fov by
+ * more than 1e-4; else 0 (and -1 on a NULL argument). */
+int32_t kt_should_render(const kt_view_state* s, const kt_view* v);
+/* App::update_render_if_needed (src/app.rs:157-182): when kt_should_render, builds the camera
+ * (kt_camera_basis, kt_fov_scale) and calls kt_renderer_submit_render; a submitted frame makes
+ * v the new prev view.  *submitted = 1 when a frame was submitted. */
+kt_status kt_renderer_submit_view(kt_renderer* r, kt_view_state* s, const kt_view* v, int32_t* submitted);
+/* The first-frame writer (src/app.rs:219-236): 0x00RRGGBB pixels, rows top to bottom, as an
+ * RGBA8 PNG with alpha 255 (stored deflate blocks).  Like the reference it does not replace an
+ * existing file: *written = 0 then, 1 when the file was written. */
+kt_status kt_write_png(const char* path, const uint32_t* pixels, uint32_t width, uint32_t height,
+                       int32_t* written);
 
 /* ---- differentiable trace (discrete adjoint) ------------------------------------------------
  * No counterpart in the reference (its renderer is forward only).  The image is the linear HDR

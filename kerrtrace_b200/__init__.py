@@ -126,6 +126,19 @@ class KtJob(C.Structure):
     _fields_ = [("cfg", KtConfig), ("cam", KtCamera), ("hdr_out", C.c_void_p), ("err_word", C.c_void_p)]
 
 
+class KtView(C.Structure):
+    """Mirror of ``kt_view``: camera position, yaw / pitch / fov in degrees (src/app.rs)."""
+
+    _fields_ = [("cam_pos", C.c_float * 3), ("yaw_deg", C.c_float), ("pitch_deg", C.c_float),
+                ("fov_deg", C.c_float)]
+
+
+class KtViewState(C.Structure):
+    """Mirror of ``kt_view_state``: the last submitted view and whether a frame exists."""
+
+    _fields_ = [("prev", KtView), ("has_frame", C.c_int32)]
+
+
 class KtError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"kerrtrace status {status}: {message}")
@@ -158,6 +171,8 @@ SIGNATURES = [
     ("kt_trace", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p]),
     ("kt_trace_counted", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p,
                                    C.POINTER(KtTraceStats), C.c_void_p]),
+    ("kt_trace_progressive", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_uint32, C.c_uint32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_context_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
     ("kt_context_get_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
     ("kt_renderer_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
@@ -195,6 +210,11 @@ SIGNATURES = [
     ("kt_renderer_set_schedule", C.c_int, [C.c_void_p, C.c_int32]),
     ("kt_renderer_frame_hdr", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("kt_renderer_destroy", None, [C.c_void_p]),
+    ("kt_view_state_init", C.c_int, [C.POINTER(KtViewState), C.POINTER(KtView)]),
+    ("kt_should_render", C.c_int32, [C.POINTER(KtViewState), C.POINTER(KtView)]),
+    ("kt_renderer_submit_view", C.c_int, [C.c_void_p, C.POINTER(KtViewState), C.POINTER(KtView),
+                                          C.POINTER(C.c_int32)]),
+    ("kt_write_png", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_int32)]),
 ]
 
 
@@ -323,6 +343,13 @@ class Context:
         check(lib().kt_trace_counted(self.handle, C.c_void_p(stream), C.byref(cam), schedule, C.c_void_p(hdr_ptr),
                                      C.c_void_p(err_ptr), C.byref(st), C.c_void_p(aux_ptr or None)))
         return st
+
+    def trace_progressive(self, cam: KtCamera, first_sample: int, n_samples: int, accum_ptr: int, hdr_ptr: int,
+                          err_ptr: int, stream: int = 0):
+        """Samples [first_sample, first_sample + n_samples) added to the running sum in accum;
+        hdr = the image of all samples so far."""
+        check(lib().kt_trace_progressive(self.handle, C.c_void_p(stream), C.byref(cam), first_sample, n_samples,
+                                         C.c_void_p(accum_ptr), C.c_void_p(hdr_ptr), C.c_void_p(err_ptr)))
 
     def set_tuning(self, schedule: int = SCHED_WAVEFRONT, block_x: int = 0, block_y: int = 0,
                    blocks_per_sm: int = 4, refill_min: int = 1, order: int = 0):
@@ -503,6 +530,12 @@ class Renderer:
     def wait(self):
         check(lib().kt_renderer_wait(self.handle))
 
+    def submit_view(self, state: "ViewState", view: KtView) -> bool:
+        """App::update_render_if_needed: submits when the view changed enough (or no frame yet)."""
+        sub = C.c_int32(0)
+        check(lib().kt_renderer_submit_view(self.handle, C.byref(state.s), C.byref(view), C.byref(sub)))
+        return bool(sub.value)
+
     def frame_hdr_ptr(self, index: int) -> int:
         p = C.c_void_p()
         check(lib().kt_renderer_frame_hdr(self.handle, index, C.byref(p)))
@@ -521,3 +554,33 @@ class Renderer:
 
 
 __all__ = [n for n in dir() if not n.startswith("_")]
+
+
+def make_view(cam_pos, yaw_deg: float, pitch_deg: float, fov_deg: float) -> KtView:
+    return KtView((C.c_float * 3)(*cam_pos), yaw_deg, pitch_deg, fov_deg)
+
+
+class ViewState:
+    """The app's record of the last submitted view (src/app.rs:25-34, 43-56)."""
+
+    def __init__(self, initial: KtView):
+        self.s = KtViewState()
+        check(lib().kt_view_state_init(C.byref(self.s), C.byref(initial)))
+
+    def should_render(self, view: KtView) -> bool:
+        r = lib().kt_should_render(C.byref(self.s), C.byref(view))
+        if r < 0:
+            raise KtError(KT_ERR_INVALID_ARG, "NULL argument")
+        return bool(r)
+
+
+def write_png(path, pixels, width: int, height: int) -> bool:
+    """First-frame writer: 0x00RRGGBB u32 pixels (numpy, row-major) -> RGBA8 PNG.  Returns False
+    when the file already exists (it is not replaced)."""
+    import numpy as np
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    if px.size != width * height:
+        raise ValueError("pixel count does not match the size")
+    done = C.c_int32(0)
+    check(lib().kt_write_png(str(path).encode(), px.ctypes.data_as(C.c_void_p), width, height, C.byref(done)))
+    return bool(done.value)

@@ -528,6 +528,9 @@ kt_status fill_scene(kt_context* c) {
     s.cutoff_gt = float_floor(d_cut);
     const float inv_spp = 1.0f / (float)cfg.spp;
     s.final_scale = (float)(d_exposure * (double)inv_spp);
+    s.sample_first = 0;
+    s.pixel_centre = (cfg.mode == KT_MODE_SPEC && cfg.spp == 1) ? 1 : 0;
+    s.accum = nullptr;
     s.temp_scale = d_temp;
     s.wl_step = d_wl;
     s.sky_intensity = d_sky;
@@ -789,6 +792,28 @@ kt_status kt_trace_counted(kt_context* ctx, void* stream, const kt_camera* cam, 
     stats->rhs_evals = h[3];
     stats->frozen_rays = h[4];
     stats->fp64_steps = h[5];
+    return KT_OK;
+}
+
+kt_status kt_trace_progressive(kt_context* ctx, void* stream, const kt_camera* cam, uint32_t first_sample,
+                               uint32_t n_samples, float* accum, float* hdr_out, uint32_t* err_word) {
+    if (!ctx || !cam || !accum || !hdr_out || !err_word) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (n_samples == 0) return fail(KT_ERR_INVALID_ARG, "n_samples must be at least 1");
+    if ((uint64_t)first_sample + n_samples > (uint64_t)std::numeric_limits<int32_t>::max())
+        return fail(KT_ERR_INVALID_ARG, "sample range out of i32 range");
+    DeviceGuard g(ctx->device);
+    ktd::Scene sc = ctx->scene;
+    sc.sample_first = (int)first_sample;
+    sc.spp = (int)n_samples;
+    sc.pixel_centre = 0;
+    sc.accum = reinterpret_cast<float4*>(accum);
+    // kernel.cu:105,136 for the total sample count so far
+    const float inv_spp = 1.0f / (float)(first_sample + n_samples);
+    sc.final_scale = (float)(define_value(ctx->cfg.exposure_scale) * (double)inv_spp);
+    const cudaError_t e = ktd::launch_trace(sc, to_camera(cam), KT_SCHED_PLAIN, reinterpret_cast<float4*>(hdr_out),
+                                            err_word, ctx->queue, nullptr, nullptr, ctx->tuning, plain_bx(ctx),
+                                            plain_by(ctx), nullptr, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "trace launch");
     return KT_OK;
 }
 

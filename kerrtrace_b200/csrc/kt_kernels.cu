@@ -209,11 +209,20 @@ __global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
         if (px >= sc.width || py >= sc.height) return;
     }
     float acc[3] = {0.0f, 0.0f, 0.0f};
+    const int pix = py * sc.width + px;
+    if (sc.accum && sc.sample_first > 0) {  // progressive: continue the running sum
+        const float4 a = sc.accum[pix];
+        acc[0] = a.x;
+        acc[1] = a.y;
+        acc[2] = a.z;
+    }
     Tally total;
     total.clear();
-    for (int smp = 0; smp < sc.spp; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total, aux);
+    const int s_end = sc.sample_first + sc.spp;
+    for (int smp = sc.sample_first; smp < s_end; ++smp) run_ray<R, MODE, COUNT>(px, py, smp, sc, cam, err, acc, total, aux);
+    if (sc.accum) sc.accum[pix] = make_float4(acc[0], acc[1], acc[2], (float)s_end);
     const float fs = sc.final_scale;
-    hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+    hdr[pix] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
     if (COUNT) add_tally(ctr, (uint64_t)sc.spp, total);
 }
 

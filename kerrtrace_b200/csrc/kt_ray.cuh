@@ -78,7 +78,7 @@ template <int MODE>
 __device__ __forceinline__ void pixel_ray(int px, int py, int sample, const Scene& sc,
                                           const Camera& cam, float dir[3]) {
     float jx, jy;
-    if (MODE == 1 && sc.spp == 1) {
+    if (MODE == 1 && sc.pixel_centre) {
         jx = 0.5f;
         jy = 0.5f;
     } else {

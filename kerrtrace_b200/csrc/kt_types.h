@@ -52,6 +52,13 @@ struct Scene {
     const double* disk_lut_d;
     float spec_tol_floor;// stated physics: tolerance never drops below base_tol * this
     int width, height;
+    // Samples: the kernel traces samples [sample_first, sample_first + spp) of each pixel.
+    // pixel_centre: stated physics with one sample per pixel uses the pixel centre.  accum
+    // (progressive sampling, plain schedule): the running sum of the raw sample colours per
+    // pixel, read when sample_first > 0 and written back with the sample count in w.
+    int sample_first;
+    int pixel_centre;
+    float4* accum;
 };
 
 struct Camera {
