@@ -61,6 +61,7 @@ def parse():
                     help="arithmetic of the main loop (mixed / fp64 need --mode spec)")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-c3", action="store_true", help="skip the 4096^2 x 8-draw precision ablation")
+    ap.add_argument("--no-sequence", action="store_true", help="skip the headless frame-sequence leg")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -364,6 +365,63 @@ def c3_run(local, tol: float, draws: int = 8, size: int = 4096) -> dict:
     return out
 
 
+def sequence_leg(cfg, tuning, local, moving: int = 60, resting: int = 30) -> dict:
+    """Headless frame sequence through the app's loop (src/app.rs:141-198, 200-260): the c2
+    observer orbits the hole by 0.5 degrees of azimuth per tick for `moving` ticks, then rests
+    for `resting` ticks, when the re-render policy submits nothing.  Two frames in flight; each
+    finished frame is handed back and the first one is written as PNG (app.rs:219-236).
+    Reports frames rendered, ticks skipped, wall time, frames per second and Mrays/s."""
+    import os
+    import tempfile
+
+    import kerrtrace_b200 as kt
+
+    views = [kt.orbit_view(100.0, 85.0, 25.0, 0.5 * k) for k in range(moving)]
+    views += [views[-1]] * resting
+    r = kt.Renderer(cfg, local)
+    r.set_tuning(tuning)
+    state = kt.ViewState(views[0])
+    png = os.path.join(tempfile.mkdtemp(prefix="kt_seq_"), "first_frame.png")
+    rendered = skipped = done = 0
+    first = None
+
+    def hand_back(block: bool) -> bool:
+        nonlocal done, first
+        while True:
+            f = r.ready_frame()
+            if f is not None:
+                if first is None:
+                    first = f[1].copy()
+                r.finish_frame(f[0])
+                done += 1
+                return True
+            if not block:
+                return False
+
+    t0 = time.perf_counter()
+    for v in views:
+        if not state.should_render(v):
+            skipped += 1
+        while state.should_render(v):
+            if r.submit_view(state, v):
+                rendered += 1
+                break
+            hand_back(True)
+        hand_back(False)
+    while done < rendered:
+        hand_back(True)
+    wall = time.perf_counter() - t0
+    r.close()
+    written = kt.write_png(png, first, cfg.width, cfg.height)
+    size = os.path.getsize(png)
+    os.remove(png)
+    os.rmdir(os.path.dirname(png))
+    rays = rendered * cfg.width * cfg.height * cfg.spp
+    return {"ticks": len(views), "frames_rendered": rendered, "ticks_skipped": skipped,
+            "wall_ms": round(wall * 1e3, 2), "frames_per_s": round(rendered / wall, 1),
+            "mrays_s": round(rays / wall / 1e6, 1), "first_frame_png_bytes": size if written else 0}
+
+
 def batch_leg(local, reps: int) -> dict:
     """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
     random spins, inclinations, observer and disk radii): one batched launch, the same launch
@@ -602,6 +660,8 @@ def run_ours(args, rank, world, local):
         line["autotune"] = tuned.summary()
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision"] = precision_leg(cfg, cam, local, max(3, args.steps))
+    if rank == 0 and world == 1 and not args.no_sequence:
+        line["sequence"] = sequence_leg(cfg, ctx.tuning(), local)
     if rank == 0 and world == 1 and not args.no_c3:
         line["c3"] = c3_leg(local)
     if rank == 0 and world == 1 and not args.no_batch:

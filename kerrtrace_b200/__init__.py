@@ -297,16 +297,27 @@ def make_camera(pos, yaw_deg: float, pitch_deg: float, fov_deg: float) -> KtCame
     return cam
 
 
-def orbit_camera(r_obs: float, incl_deg: float, fov_deg: float, azimuth_deg: float = 0.0) -> KtCamera:
-    """Observer at Kerr-Schild radius r_obs, inclination from the spin axis (+y), looking at the
-    hole.  Azimuth 0 puts the camera in the x-y plane; yaw/pitch follow src/math.rs:3-14."""
+def _orbit(r_obs: float, incl_deg: float, azimuth_deg: float):
     i = math.radians(incl_deg)
     az = math.radians(azimuth_deg)
     pos = (r_obs * math.sin(i) * math.cos(az), r_obs * math.cos(i), r_obs * math.sin(i) * math.sin(az))
     d = [-p / r_obs for p in pos]
     pitch = math.degrees(math.asin(max(-1.0, min(1.0, d[1]))))
     yaw = math.degrees(math.atan2(d[0], -d[2]))
+    return pos, yaw, pitch
+
+
+def orbit_camera(r_obs: float, incl_deg: float, fov_deg: float, azimuth_deg: float = 0.0) -> KtCamera:
+    """Observer at Kerr-Schild radius r_obs, inclination from the spin axis (+y), looking at the
+    hole.  Azimuth 0 puts the camera in the x-y plane; yaw/pitch follow src/math.rs:3-14."""
+    pos, yaw, pitch = _orbit(r_obs, incl_deg, azimuth_deg)
     return make_camera(pos, yaw, pitch, fov_deg)
+
+
+def orbit_view(r_obs: float, incl_deg: float, fov_deg: float, azimuth_deg: float = 0.0) -> "KtView":
+    """The same observer as the app holds it (position, yaw, pitch, fov)."""
+    pos, yaw, pitch = _orbit(r_obs, incl_deg, azimuth_deg)
+    return make_view(pos, yaw, pitch, fov_deg)
 
 
 # ---- device objects -----------------------------------------------------------------------
