@@ -121,7 +121,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
         sm = sorted(x[0] for x in self.samples)
         reasons = sorted({name for _, why, _ in self.samples for bit, name in self.REASONS.items() if why & bit})
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": reasons,
+        return {"sm_mhz": sm[len(sm) // 2], "sm_mhz_min": sm[0], "sm_max_mhz": self.max_mhz, "reasons": reasons,
                 "power_w_max": round(max(x[2] for x in self.samples), 1), "samples": len(self.samples)}
 
 
@@ -658,16 +658,18 @@ def run_ours(args, rank, world, local):
     }
     if tuned is not None:
         line["autotune"] = tuned.summary()
-    if rank == 0 and world == 1 and not args.no_precision:
-        line["precision"] = precision_leg(cfg, cam, local, max(3, args.steps))
-    if rank == 0 and world == 1 and not args.no_sequence:
-        line["sequence"] = sequence_leg(cfg, ctx.tuning(), local)
-    if rank == 0 and world == 1 and not args.no_c3:
-        line["c3"] = c3_leg(local)
-    if rank == 0 and world == 1 and not args.no_batch:
-        line["batch"] = batch_leg(local, 3)
-    if rank == 0 and world == 1 and not args.no_adjoint:
-        line["adjoint"] = adjoint_leg(local, max(3, args.steps))
+    # legs, each with the SM clock sampled while it runs; the long 4096^2 ablation goes last, so
+    # that the heat it leaves does not lower the clocks of the shorter legs
+    legs = [("precision", args.no_precision, lambda: precision_leg(cfg, cam, local, max(3, args.steps))),
+            ("adjoint", args.no_adjoint, lambda: adjoint_leg(local, max(3, args.steps))),
+            ("batch", args.no_batch, lambda: batch_leg(local, 3)),
+            ("sequence", args.no_sequence, lambda: sequence_leg(cfg, ctx.tuning(), local)),
+            ("c3", args.no_c3, lambda: c3_leg(local))]
+    for name, skip, run in legs:
+        if rank == 0 and world == 1 and not skip:
+            with ClockSampler(local, period_s=0.02) as clk:
+                line[name] = run()
+            line[name]["clocks"] = clk.summary()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, cam, args.cpu_seconds)
     if rank == 0:
