@@ -14,7 +14,7 @@ radius 24, ACES + sRGB): the trace kernel plus the post-processing kernel.
           handed back
   roofline  FP32 work of the trace kernel (counted RHS evaluations / attempts / steps x the
           static op counts in kerrtrace_b200/flops.py) / its event-timed duration, against the
-          FP32 FMA peak at the SM clock sampled during the run (148 SMs x 128 lanes x 2 flops)
+          FP32 FMA throughput measured on the same GPU before the timed region (kt_fma_peak)
   cpu_baseline  the CPU oracle (f64 restatement, all host cores) on a strided sample of the
           same frame
 
@@ -554,6 +554,10 @@ def run_ours(args, rank, world, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
 
+    try:  # the FP32 roofline's denominator, measured on this GPU before the timed region
+        measured_fma = kt.fma_peak(local, 16384)
+    except kt.KtError:
+        measured_fma = None
     tuned = autotune.autotune(ctx, cam, stream=stream) if sched == kt.SCHED_AUTO else None
     stats = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), stream, sched)
     work = flops.trace_flops(stats)
@@ -622,15 +626,18 @@ def run_ours(args, rank, world, local):
     achieved = work / (trace_ms / 1e3) / 1e12
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     mhz = clocks.get("sm_mhz") or 1965.0
-    peak = sms * flops.FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+    nominal = sms * flops.FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+    peak = measured_fma[0] if measured_fma else nominal
     t = ctx.tuning()
     kernel = "trace_plain_kernel" if (t.schedule == kt.SCHED_PLAIN and sched == kt.SCHED_AUTO) or sched == kt.SCHED_PLAIN \
         else "trace_wavefront_kernel"
     roofline = {"bound": "fp32", "kernel": kernel,
                 "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4),
-                "peak_source": f"FP32 FMA peak at the sampled median SM clock ({mhz:.0f} MHz): "
-                               f"{sms} SMs x 128 lanes x 2 flops",
+                "peak_source": ("measured: FP32 FMA throughput of this GPU (kt_fma_peak: 8 independent FMA "
+                                f"chains per thread on every SM, best of 5 launches of {measured_fma[1]:.3f} ms)")
+                if measured_fma else f"nominal: {sms} SMs x 128 lanes x 2 flops at the sampled clock",
+                "nominal_at_clock": round(nominal, 3),
                 "traffic": int(TRACE_TRAFFIC_PER_RAY * n * cfg.spp),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one trace launch "
                                   "(c2 scene at 960x540: 149504 + 0 B), scaled to this launch by its rays",

@@ -336,6 +336,12 @@ kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning);
 kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev);
 void kt_renderer_destroy(kt_renderer* r);
 
+/* ---- measurement ---------------------------------------------------------------------------- */
+/* FP32 FMA throughput of `device` in TFLOP/s (the denominator of the trace's roofline): a
+ * kernel of 8 independent FMA chains of `iters` steps per thread, 512-thread blocks filling
+ * every SM, best of 5 timed launches (CUDA events) after one warm-up.  Synchronises. */
+kt_status kt_fma_peak(int device, uint32_t iters, double* tflops, float* ms);
+
 /* ---- headless mirror of the interactive loop's render policy (src/app.rs) ------------------ */
 /* A camera as the app holds it: position, yaw and pitch in degrees, vertical fov in degrees. */
 typedef struct kt_view {

@@ -215,6 +215,7 @@ SIGNATURES = [
     ("kt_renderer_submit_view", C.c_int, [C.c_void_p, C.POINTER(KtViewState), C.POINTER(KtView),
                                           C.POINTER(C.c_int32)]),
     ("kt_write_png", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_int32)]),
+    ("kt_fma_peak", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
 ]
 
 
@@ -595,3 +596,11 @@ def write_png(path, pixels, width: int, height: int) -> bool:
     done = C.c_int32(0)
     check(lib().kt_write_png(str(path).encode(), px.ctypes.data_as(C.c_void_p), width, height, C.byref(done)))
     return bool(done.value)
+
+
+def fma_peak(device: int = 0, iters: int = 4096) -> tuple[float, float]:
+    """Measured FP32 FMA throughput of the device: (TFLOP/s, ms of the best launch)."""
+    tf = C.c_double(0.0)
+    ms = C.c_float(0.0)
+    check(lib().kt_fma_peak(device, iters, C.byref(tf), C.byref(ms)))
+    return tf.value, ms.value

@@ -817,6 +817,52 @@ kt_status kt_trace_progressive(kt_context* ctx, void* stream, const kt_camera* c
     return KT_OK;
 }
 
+kt_status kt_fma_peak(int device, uint32_t iters, double* tflops, float* ms) {
+    if (!tflops) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (iters == 0 || iters > (1u << 24)) return fail(KT_ERR_INVALID_ARG, "iters out of range");
+    DeviceGuard g(device);
+    int sms = 0, per_sm = 0;
+    KT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    KT_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device), "threads per SM");
+    const int blocks = sms * std::max(1, per_sm / 512);
+    float* sink = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t st = nullptr;
+    kt_status out = KT_OK;
+    float best = 0.0f;
+    do {
+        cudaError_t e;
+        if ((e = cudaMalloc(&sink, sizeof(float))) != cudaSuccess || (e = cudaEventCreate(&e0)) != cudaSuccess ||
+            (e = cudaEventCreate(&e1)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = ktd::launch_fma_probe(blocks, (int)iters, sink, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            out = cuda_fail(e, "FMA probe");
+            break;
+        }
+        for (int rep = 0; rep < 5 && out == KT_OK; ++rep) {
+            float t = 0.0f;
+            if ((e = cudaEventRecord(e0, st)) != cudaSuccess ||
+                (e = ktd::launch_fma_probe(blocks, (int)iters, sink, st)) != cudaSuccess ||
+                (e = cudaEventRecord(e1, st)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess ||
+                (e = cudaEventElapsedTime(&t, e0, e1)) != cudaSuccess) {
+                out = cuda_fail(e, "FMA probe timing");
+                break;
+            }
+            if (best == 0.0f || t < best) best = t;
+        }
+    } while (false);
+    if (sink) cudaFree(sink);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    if (out != KT_OK) return out;
+    const double flops = 16.0 * (double)iters * (double)blocks * 512.0;
+    *tflops = flops / ((double)best * 1e-3) / 1e12;
+    if (ms) *ms = best;
+    return KT_OK;
+}
+
 kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom) {
     if (!ctx || !hdr || !bloom) return fail(KT_ERR_INVALID_ARG, "NULL argument");
     DeviceGuard g(ctx->device);

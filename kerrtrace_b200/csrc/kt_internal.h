@@ -70,6 +70,9 @@ cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const f
 // Both post passes; scratch: a width x height float4 bloom buffer (unused when bloom is off).
 cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image, float4* scratch,
                               cudaStream_t stream);
+// FP32 FMA throughput probe: `blocks` x 512 threads, each running 8 independent FMA chains of
+// `iters` steps (16 * iters flops per thread).
+cudaError_t launch_fma_probe(int blocks, int iters, float* sink, cudaStream_t st);
 
 }  // namespace ktd
 

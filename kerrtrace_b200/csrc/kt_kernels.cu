@@ -740,6 +740,29 @@ cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const f
     return cudaGetLastError();
 }
 
+// FP32 FMA throughput probe (the denominator of the trace's roofline): eight independent
+// dependent chains per thread hide the FMA latency; the chains are kept alive by a store that
+// only a sum of exactly 12345.678 would trigger.
+__global__ void __launch_bounds__(512) fma_probe_kernel(float b, float c, int iters, float* sink) {
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = (float)threadIdx.x * 1e-3f + (float)i;
+#pragma unroll 8
+    for (int k = 0; k < iters; ++k) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = fmaf(v[i], b, c);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += v[i];
+    if (s == 12345.678f) sink[0] = s;
+}
+
+cudaError_t launch_fma_probe(int blocks, int iters, float* sink, cudaStream_t st) {
+    fma_probe_kernel<<<blocks, 512, 0, st>>>(0.999999f, 1e-6f, iters, sink);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t* image, float4* scratch,
                               cudaStream_t st) {
     if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
