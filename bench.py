@@ -125,17 +125,22 @@ class ClockSampler:
                 "power_w_max": round(max(x[2] for x in self.samples), 1), "samples": len(self.samples)}
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from torchrun).  The
+    process group only carries the barrier and the max-over-ranks time; `gloo` runs the same
+    host logic on CPU (tests)."""
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    if backend == "nccl":
+        torch.cuda.set_device(local)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
     return rank, world, local
 
 
@@ -150,9 +155,16 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_mrays_s(rays_per_rank: int, world: int, max_ms: float) -> float:
+    """Whole-job throughput: the rays of all ranks over the slowest rank's time (weak scaling:
+    every rank traces its own frame of the same size)."""
+    return rays_per_rank * world / (max_ms / 1e3) / 1e6
 
 
 def rank_camera(kt, workloads, name, rank, world, size=None):
@@ -591,7 +603,7 @@ def run_ours(args, rank, world, local):
     t_post = [b.elapsed_time(c) for _, b, c in ev]
     total_ms = max_over_ranks(sum(t_steps), world)
     rays_all = n * cfg.spp * world * args.steps
-    value = rays_all / (total_ms / 1e3) / 1e6
+    value = job_mrays_s(n * cfg.spp * args.steps, world, total_ms)
 
     # end to end through the renderer API (host buffers), same launch shape
     rend = kt.Renderer(cfg, local)
