@@ -24,6 +24,7 @@ import numpy as np
 from . import ORDER_LONG_FIRST, ORDER_TILES, SCHED_AUTO, SCHED_PLAIN, SCHED_WAVEFRONT, Context, KtCamera
 
 PLAIN_BLOCKS = [(16, 16), (32, 8), (8, 8), (16, 8), (32, 4), (8, 16)]
+PLAIN_BLOCKS_128 = [(16, 8), (8, 16), (32, 4)]
 WAVE_BLOCKS_PER_SM = [3, 4, 5, 6]
 WAVE_REFILL = [1, 4, 8, 16]
 
@@ -33,6 +34,9 @@ def candidates(precision: int = 0, mode: int = 0) -> list[dict]:
     for order in (ORDER_TILES, ORDER_LONG_FIRST):
         out += [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=4, refill_min=1, order=order)
                 for bx, by in PLAIN_BLOCKS]
+        if precision != 2:  # 128-thread blocks with 5 or 6 resident per SM (FP32 and mixed)
+            out += [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=b, refill_min=1, order=order)
+                    for bx, by in PLAIN_BLOCKS_128 for b in (5, 6)]
         # only the FP32 reference-semantics kernel has the 3/5/6 blocks-per-SM variants
         bps = WAVE_BLOCKS_PER_SM if (precision == 0 and mode == 0) else [4]
         out += [dict(schedule=SCHED_WAVEFRONT, block_x=0, block_y=0, blocks_per_sm=b, refill_min=r, order=order)

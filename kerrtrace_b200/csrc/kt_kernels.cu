@@ -186,11 +186,13 @@ __global__ void __launch_bounds__(256) rank_pixels_kernel(const Scene sc, const 
 
 // Resident 256-thread blocks per SM asked of the compiler for the plain kernel: two for the
 // FP32 and mixed paths (at most 128 registers per thread, 16 warps per SM), one for FP64.
+// Blocks of at most 128 threads can also ask for 5 or 6 resident blocks (at most 102 or 85
+// registers: 20 or 24 warps per SM), a choice of the tuning (blocks_per_sm) for FP32 and mixed.
 template <class R> struct PlainMinBlocks { static constexpr int v = 2; };
 template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
 
-template <class R, int MODE, bool COUNT, int MAXT>
-__global__ void __launch_bounds__(MAXT, MAXT == 256 ? PlainMinBlocks<R>::v : 1)
+template <class R, int MODE, bool COUNT, int MAXT, int MINB = (MAXT == 256 ? PlainMinBlocks<R>::v : 1)>
+__global__ void __launch_bounds__(MAXT, MINB)
     trace_plain_kernel(const __grid_constant__ Scene sc, const Camera cam,
                                                            float4* __restrict__ hdr,
                                                            uint32_t* __restrict__ err,
@@ -327,12 +329,22 @@ template <> struct WaveDefaults<Mixed> { static constexpr int minb = 4; };
 
 template <class R, int MODE, bool COUNT>
 static cudaError_t launch_plain(const Scene& sc, const Camera& cam, float4* hdr, uint32_t* err,
-                                unsigned long long* ctr, float4* aux, int bx, int by, const unsigned* order,
-                                cudaStream_t st) {
+                                unsigned long long* ctr, float4* aux, int bx, int by, int minb,
+                                const unsigned* order, cudaStream_t st) {
     const dim3 block(bx, by);
     const unsigned n = (unsigned)sc.width * (unsigned)sc.height, per = (unsigned)(bx * by);
     const dim3 grid = order ? dim3((n + per - 1) / per)
                             : dim3((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
+    if constexpr (!std::is_same<R, double>::value) {
+        if (bx * by <= 128 && minb == 5) {
+            trace_plain_kernel<R, MODE, COUNT, 128, 5><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
+            return cudaGetLastError();
+        }
+        if (bx * by <= 128 && minb == 6) {
+            trace_plain_kernel<R, MODE, COUNT, 128, 6><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
+            return cudaGetLastError();
+        }
+    }
     if (bx * by <= 256)
         trace_plain_kernel<R, MODE, COUNT, 256><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
     else
@@ -388,8 +400,8 @@ static cudaError_t launch_typed(const Scene& sc, const Camera& cam, int schedule
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (schedule == 0)
-        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, aux, bx, by, order, st)
-                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, aux, bx, by, order, st);
+        return ctr ? launch_plain<R, MODE, true>(sc, cam, hdr, err, ctr, aux, bx, by, tn.blocks_per_sm, order, st)
+                   : launch_plain<R, MODE, false>(sc, cam, hdr, err, ctr, aux, bx, by, tn.blocks_per_sm, order, st);
     return ctr ? launch_wave<R, MODE, true>(sc, cam, hdr, err, queue, ctr, aux, tn, order, st)
                : launch_wave<R, MODE, false>(sc, cam, hdr, err, queue, ctr, aux, tn, order, st);
 }
