@@ -125,12 +125,67 @@ __device__ __forceinline__ R ks_radius(R x, R y, R z, R aa) {
 // (cuda/kerr_math.cuh:97); differentiating r^2 = (u + s)/2 with u = rho^2 - a^2 and
 // s^2 = u^2 + 4 a^2 y^2 gives y (1 + (u + 2a^2)/s).  Reference mode keeps the reference's
 // expression (the drop-in reproduces its images); stated-physics mode uses the exact one.
+//
+// Stated physics (EXACT) evaluates the same exact gradient in a shorter form.  With r_i = dr/dx_i,
+// D = r^2 + a^2, N_x = r x - a z, N_z = r z + a x (l_x = N_x / D, l_z = N_z / D, l_y = y / r) and
+// lp = l.p - pt, the momentum derivative of l.p is a multiple of grad r plus three direct terms,
+//   d(l.p)/dx_i = r_i c + (r p_x + a p_z) / D [i = x], p_y / r [i = y], (r p_z - a p_x) / D [i = z],
+//   c = (x p_x + z p_z) / D - 2 r (N_x p_x + N_z p_z) / D^2 - p_y y / r^2,
+// and dHk/dx_i = r_i e - [i = y] f with e = M r^2 (3 a^2 y^2 - r^4) / denH^2 and
+// f = 2 M a^2 y r^3 / denH^2 (denH = r^4 + a^2 y^2), so that
+//   dp_i/dl = r_i (e lp^2 + 2 Hk lp c) - [i = y] f lp^2 + 2 Hk lp (direct term)_i,
+// instead of the full 3 x 3 Jacobian of l that the reference form builds (about 40% fewer
+// operations per evaluation).
 template <class R, bool EXACT>
 __device__ __forceinline__ void hamilton_rhs(const R* __restrict__ st, R pt, R a, R aa, R M,
                                              R* __restrict__ d) {
     using O = Ops<R>;
     const R x = st[0], y = st[1], z = st[2];
     const R px = st[3], py = st[4], pz = st[5];
+    if constexpr (EXACT) {
+        const R rho2 = O::fma(x, x, O::fma(y, y, z * z));
+        const R u = rho2 - aa;
+        const R aay2 = aa * y * y;
+        const R s_sq = O::fma(u, u, R(4) * aay2);
+        const R inv_s = O::rsq(s_sq);
+        const R r2 = R(0.5) * O::fma(s_sq, inv_s, u);
+        const R inv_r = O::rsq(r2);
+        const R r = r2 * inv_r;
+        const R half_inv_r = R(0.5) * inv_r;
+        const R gxz = O::fma(u, inv_s, R(1)) * half_inv_r;     // r_x / x = r_z / z
+        const R rx = x * gxz;
+        const R rz = z * gxz;
+        const R ry = y * (O::fma(u + R(2) * aa, inv_s, R(1)) * half_inv_r);
+        const R den = r2 + aa;
+        const R inv_den = O::fdiv(R(1), den);
+        const R Nx = O::fma(r, x, -a * z);
+        const R Nz = O::fma(r, z, a * x);
+        const R lx = Nx * inv_den;
+        const R ly = y * inv_r;
+        const R lz = Nz * inv_den;
+        const R r3 = r2 * r;
+        const R denH = O::fma(r2, r2, aay2);
+        const R inv_denH = O::fdiv(R(1), denH);
+        const R Hk = M * r3 * inv_denH;
+        const R lp = O::fma(lx, px, O::fma(ly, py, O::fma(lz, pz, -pt)));
+        const R two_H_lp = R(2) * Hk * lp;
+        d[0] = O::fma(-two_H_lp, lx, px);
+        d[1] = O::fma(-two_H_lp, ly, py);
+        d[2] = O::fma(-two_H_lp, lz, pz);
+        const R A = O::fma(px, x, pz * z);
+        const R B = O::fma(px, Nx, pz * Nz);
+        const R c = O::fma(A - R(2) * r * B * inv_den, inv_den, -py * ly * inv_r);
+        const R ih2 = inv_denH * inv_denH;
+        const R e = M * r2 * O::fma(R(3), aay2, -r2 * r2) * ih2;
+        const R f = R(2) * M * aa * y * r3 * ih2;
+        const R lp2 = lp * lp;
+        const R Q = O::fma(e, lp2, two_H_lp * c);
+        const R tw = two_H_lp * inv_den;
+        d[3] = O::fma(rx, Q, tw * O::fma(r, px, a * pz));
+        d[4] = O::fma(ry, Q, O::fma(-f, lp2, two_H_lp * py * inv_r));
+        d[5] = O::fma(rz, Q, tw * O::fma(r, pz, -a * px));
+        return;
+    }
     const R rho2 = O::fma(x, x, O::fma(y, y, z * z));
     const R u = rho2 - aa;
     const R s_sq = O::fma(u, u, R(4) * aa * y * y);
