@@ -436,8 +436,9 @@ def sequence_leg(cfg, tuning, local, moving: int = 60, resting: int = 30) -> dic
 
 def batch_leg(local, reps: int) -> dict:
     """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
-    random spins, inclinations, observer and disk radii): one batched launch, the same launch
-    replayed from a CUDA graph, and the baseline of 64 sequential plain launches."""
+    random spins, inclinations, observer and disk radii): one batched launch at the fastest of
+    six block shapes, the same launch replayed from a CUDA graph, and the baseline of 64
+    sequential plain launches."""
     import torch
 
     import kerrtrace_b200 as kt
@@ -450,6 +451,21 @@ def batch_leg(local, reps: int) -> dict:
     rays = b.rays()
     stream = torch.cuda.current_stream().cuda_stream
     out = {"jobs": len(jobs), "rays": rays}
+    # block shape of the batched launch: the fastest of the plain shapes (one launch each)
+    shapes = {}
+    for bx, by in ((16, 16), (32, 8), (8, 8), (16, 8), (8, 16), (32, 4)):
+        b.set_block(bx, by)
+        b.trace(stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.trace(stream)
+        e1.record()
+        torch.cuda.synchronize()
+        shapes[f"{bx}x{by}"] = round(e0.elapsed_time(e1), 3)
+    best = min(shapes, key=shapes.get)
+    b.set_block(*(int(v) for v in best.split("x")))
+    out["block_ms"] = shapes
+    out["block"] = best
     for name, fn in (("sequential_plain", lambda: b.trace_sequential(stream, kt.SCHED_PLAIN)),
                      ("batched_launch", lambda: b.trace(stream)),
                      ("batched_graph", lambda: b.trace_graph(stream))):
