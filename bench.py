@@ -438,7 +438,7 @@ def batch_leg(local, reps: int) -> dict:
     """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
     random spins, inclinations, observer and disk radii): one batched launch at the fastest of
     six block shapes, the same launch replayed from a CUDA graph, and the baseline of 64
-    sequential plain launches."""
+    sequential plain launches; then the same renders in stated physics and mixed precision."""
     import torch
 
     import kerrtrace_b200 as kt
@@ -481,6 +481,25 @@ def batch_leg(local, reps: int) -> dict:
         out[name] = {"ms": round(ms, 3), "mrays_s": round(rays / ms / 1e3, 1)}
     out["speedup_graph_vs_sequential"] = round(out["sequential_plain"]["ms"] / out["batched_graph"]["ms"], 3)
     b.close()
+    # the same 64 renders in stated physics and mixed precision, one graph-replayed launch
+    mjobs = []
+    for c, cam in jobs:
+        c = c.copy()
+        c.mode, c.precision = kt.MODE_SPEC, kt.PREC_MIXED
+        mjobs.append((c, cam))
+    mb = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(mjobs, bufs)], local)
+    mb.set_block(*(int(v) for v in best.split("x")))
+    mb.trace_graph(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        mb.trace_graph(stream)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out["mixed_batched_graph"] = {"ms": round(ms, 3), "mrays_s": round(mb.rays() / ms / 1e3, 1)}
+    mb.close()
     return out
 
 
