@@ -20,8 +20,12 @@ def _alloc(torch, jobs):
     return bufs
 
 
-def test_batch_matches_per_job_traces(cuda):
+@pytest.mark.parametrize("mode,prec", [(kt.MODE_REF, kt.PREC_FP32), (kt.MODE_SPEC, kt.PREC_MIXED),
+                                       (kt.MODE_SPEC, kt.PREC_FP64)])
+def test_batch_matches_per_job_traces(cuda, mode, prec):
     jobs = workloads.c4_jobs(scale=16)[::8]   # 8 jobs of different sizes, spins, cameras, disks
+    for c, _ in jobs:
+        c.mode, c.precision = mode, prec
     bufs = _alloc(cuda, jobs)
     b = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(jobs, bufs)])
     assert b.rays() == sum(c.width * c.height for c, _ in jobs)
