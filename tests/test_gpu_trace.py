@@ -149,3 +149,33 @@ def test_long_first_order_is_bit_identical(cuda, name, mode, prec, size, schedul
         assert np.all(out[:, 3] == 1.0)
         assert np.array_equal(out.view(np.uint32), base.view(np.uint32))
         assert np.array_equal(err.cpu().numpy().view(np.uint32), eb)
+
+
+@pytest.mark.parametrize("size", [(1, 1), (1, 17), (23, 1), (37, 23)])
+def test_tiny_and_ragged_frames_match_reference_kernel(cuda, orc, size):
+    """Frames of one pixel, one row, one column and odd sizes: the trace (2 samples, noise) and
+    the fused post (bloom radius 6 wider than the frame) are bit-identical to the reference's
+    trace_kernel, bloom_horizontal and post_process on the same input."""
+    cfg, cam = workloads.scene("t1")
+    cfg = workloads.scaled(cfg, *size)
+    ours, err_o, _, ctx = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    ref, err_r = run_ref(cuda, "t1", cfg, cam)
+    assert np.array_equal(ours.view(np.uint32), ref.view(np.uint32)), size
+    assert np.array_equal(err_o, err_r)
+    n = cfg.width * cfg.height
+    hdr = cuda.tensor(ours, device="cuda")
+    img = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    ctx.post_fused(hdr.data_ptr(), img.data_ptr())
+    radius = int(np.ceil(np.float32(cfg.bloom_radius)))
+    sigma = float(np.float32(np.float32(cfg.bloom_radius) / np.float32(3.0)))
+    active = int(bool(cfg.bloom_enabled) and radius > 0 and cfg.bloom_intensity > 0)
+    k = orc.RefKernel("t1")
+    bloom_r = cuda.zeros((n, 4), device="cuda")
+    img_r = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    k.bloom(hdr.data_ptr(), bloom_r.data_ptr(), cfg, radius, sigma, active)
+    k.post(hdr.data_ptr(), bloom_r.data_ptr(), img_r.data_ptr(), cfg, radius, sigma, cfg.bloom_intensity, active)
+    cuda.cuda.synchronize()
+    assert active == 1
+    assert np.array_equal(img.cpu().numpy(), img_r.cpu().numpy()), size
+    k.close()
+    ctx.close()
