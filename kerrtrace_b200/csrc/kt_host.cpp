@@ -591,7 +591,9 @@ kt_status validate_cfg(const kt_config* cfg) {
     if (cfg->precision < KT_PREC_FP32 || cfg->precision > KT_PREC_FP64) return fail(KT_ERR_INVALID_ARG, "unknown precision %d", cfg->precision);
     if (cfg->mode == KT_MODE_REF && cfg->precision != KT_PREC_FP32)
         return fail(KT_ERR_INVALID_ARG, "reference mode runs the reference's FP32 arithmetic; use KT_MODE_SPEC for mixed/FP64");
-    if (cfg->width > 32768 || cfg->height > 32768 || (uint64_t)cfg->width * cfg->height > (1ull << 31))
+    if (cfg->width == 0 || cfg->height == 0)
+        return fail(KT_ERR_INVALID_ARG, "empty image: %ux%u", cfg->width, cfg->height);
+    if (cfg->width > 32768 || cfg->height > 32768)
         return fail(KT_ERR_INVALID_ARG, "image too large: %ux%u", cfg->width, cfg->height);
     const uint64_t bt = (uint64_t)cfg->block_dim[0] * cfg->block_dim[1];
     if (cfg->block_dim[0] == 0 || cfg->block_dim[1] == 0 || bt > 1024)

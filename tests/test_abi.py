@@ -199,6 +199,12 @@ def test_invalid_configs_rejected_before_device(kt):
     c = cfg.copy()
     c.mode, c.precision = kt.MODE_REF, kt.PREC_FP64
     assert kt.lib().kt_context_create(C.byref(c), 0, C.byref(C.c_void_p())) == kt.KT_ERR_INVALID_ARG
+    # frames beyond 32768 on a side (the pixel index stays a 32-bit int, as in the reference's
+    # kernel) and empty frames
+    for w, h in ((40000, 16), (16, 40000), (0, 16), (16, 0)):
+        c = cfg.copy()
+        c.width, c.height = w, h
+        assert kt.lib().kt_context_create(C.byref(c), 0, C.byref(C.c_void_p())) == kt.KT_ERR_INVALID_ARG, (w, h)
 
 
 def test_diff_rejects_unsupported_configurations(kt):
