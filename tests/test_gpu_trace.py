@@ -179,3 +179,22 @@ def test_tiny_and_ragged_frames_match_reference_kernel(cuda, orc, size):
     assert np.array_equal(img.cpu().numpy(), img_r.cpu().numpy()), size
     k.close()
     ctx.close()
+
+
+def test_large_frame_matches_reference_kernel(cuda):
+    """An 8192 x 8192 frame of the 1080p scene (67 M rays, 1 GB of HDR) against the reference
+    kernel (which takes about 10 s for it): all but a handful of pixels bit-identical (3 on
+    B200: two-hit rays in one small patch of the secondary image, 5e-6 apart; the cause is not
+    known), every pixel far inside the 1e-3 parity bar."""
+    cfg, cam = workloads.scene("c2")
+    cfg = workloads.scaled(cfg, 8192, 8192)
+    ours, err_o, _, ctx = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    ctx.close()
+    ref, err_r = run_ref(cuda, "c2", cfg, cam)
+    diff = np.flatnonzero((ours.view(np.uint32) != ref.view(np.uint32)).any(1))
+    print("pixels not bit-identical:", len(diff))
+    assert len(diff) <= 10
+    if len(diff):
+        a, b = ours[diff, :3].astype(np.float64), ref[diff, :3].astype(np.float64)
+        assert np.all(np.abs(a - b) <= 1e-5 * np.abs(b).max(1, keepdims=True))
+    assert np.array_equal(err_o, err_r)
