@@ -191,6 +191,16 @@ kt_status kt_generate_blackbody_lut(uint32_t size, float max_temp, float wavelen
  * Novikov-Thorne / Page-Thorne flux factor on `size` radii in [disk_inner, disk_outer]. */
 kt_status kt_generate_disk_lut(const kt_kerr_params* params, float disk_outer, uint32_t size,
                                float* out);
+/* The same two tables generated on the device, on `stream`, into device memory (dev_out:
+ * float[4*size] / float[size]), one thread per row.  They use CUDA's accurate math functions and
+ * agree with the host tables to a few ulp, not bit for bit (CUDA's and glibc's libm round
+ * differently in the last place).  For hosts that build many per-scene tables (batches) or keep
+ * everything on the device. */
+kt_status kt_generate_blackbody_lut_device(uint32_t size, float max_temp, float wavelength_start,
+                                           float wavelength_end, float wavelength_step, float* dev_out,
+                                           void* stream);
+kt_status kt_generate_disk_lut_device(const kt_kerr_params* params, float disk_outer, uint32_t size,
+                                      float* dev_out, void* stream);
 /* build_cuda_defines (src/renderer/utils.rs:121-163): the `#define` header text the reference
  * prepends to kernel.cu.  Writes a NUL-terminated string; *len gets its length. */
 kt_status kt_build_defines(const kt_config* cfg, char* buf, size_t cap, size_t* len);

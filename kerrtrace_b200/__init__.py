@@ -216,6 +216,10 @@ SIGNATURES = [
                                           C.POINTER(C.c_int32)]),
     ("kt_write_png", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_int32)]),
     ("kt_fma_peak", C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    ("kt_generate_blackbody_lut_device", C.c_int, [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
+                                                   C.c_void_p, C.c_void_p]),
+    ("kt_generate_disk_lut_device", C.c_int, [C.POINTER(KtKerrParams), C.c_float, C.c_uint32, C.c_void_p,
+                                              C.c_void_p]),
 ]
 
 
@@ -266,6 +270,18 @@ def generate_disk_lut(params: KtKerrParams, disk_outer: float, size: int):
     out = np.zeros(size, dtype=np.float32)
     check(lib().kt_generate_disk_lut(C.byref(params), disk_outer, size, out.ctypes.data))
     return out
+
+
+def generate_blackbody_lut_device(size, max_temp, wl_start, wl_end, wl_step, dev_ptr: int, stream: int = 0):
+    """The blackbody table computed on the device into dev_ptr (float[4 * size])."""
+    check(lib().kt_generate_blackbody_lut_device(size, max_temp, wl_start, wl_end, wl_step, C.c_void_p(dev_ptr),
+                                                 C.c_void_p(stream)))
+
+
+def generate_disk_lut_device(params: KtKerrParams, disk_outer: float, size: int, dev_ptr: int, stream: int = 0):
+    """The disk temperature table computed on the device into dev_ptr (float[size])."""
+    check(lib().kt_generate_disk_lut_device(C.byref(params), disk_outer, size, C.c_void_p(dev_ptr),
+                                            C.c_void_p(stream)))
 
 
 def build_defines(cfg: KtConfig) -> str:

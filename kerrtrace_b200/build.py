@@ -66,6 +66,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     log = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-use_fast_math", "-Xptxas", "-v",
                 "-Xcompiler", "-fPIC", *inc, "-c", str(CSRC / "kt_noalloc.cu"), "-o", str(n_obj)])
     (BUILD / "ptxas_kt_noalloc.txt").write_text(log)
+    l_obj = BUILD / "kt_luts.o"  # accurate libm: no fast math
+    log = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xptxas", "-v",
+                "-Xcompiler", "-fPIC", *inc, "-c", str(CSRC / "kt_luts.cu"), "-o", str(l_obj)])
+    (BUILD / "ptxas_kt_luts.txt").write_text(log)
     d_obj = BUILD / "kt_diff.o"
     log = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-use_fast_math", "-Xptxas", "-v",
                 "-Xcompiler", "-fPIC", *inc, "-c", str(CSRC / "kt_diff.cu"), "-o", str(d_obj)])
@@ -81,7 +85,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
           "-I", str(cuda_home / "include"), "-c", str(CSRC / "kt_app.cpp"), "-o", str(a_obj)])
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-cudart", "static", str(k_obj), str(n_obj), str(d_obj), str(h_obj), str(dh_obj),
-          str(a_obj), "-o", str(tmp)])
+          str(a_obj), str(l_obj), "-o", str(tmp)])
     os.replace(tmp, LIB)
     return LIB
 

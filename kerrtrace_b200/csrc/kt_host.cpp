@@ -297,6 +297,34 @@ kt_status kt_generate_blackbody_lut(uint32_t size, float max_temp, float wl_star
     return KT_OK;
 }
 
+kt_status kt_generate_blackbody_lut_device(uint32_t size, float max_temp, float wl_start, float wl_end,
+                                           float wl_step, float* dev_out, void* stream) {
+    if (!dev_out) return fail(KT_ERR_INVALID_ARG, "dev_out is NULL");
+    if (size < 2) return fail(KT_ERR_INVALID_ARG, "blackbody LUT size must be at least 2");
+    if (!std::isfinite(wl_step) || wl_step <= 0.0f)
+        return fail(KT_ERR_INVALID_ARG, "wavelength step must be positive and finite");
+    int n = 0;  // the host generator's grid: f32 accumulation from wl_start while <= wl_end
+    for (float l = wl_start; !(l > wl_end); l += wl_step)
+        if (++n > (1 << 24)) return fail(KT_ERR_INVALID_ARG, "wavelength grid too large");
+    const cudaError_t e = ktd::launch_blackbody_lut(size, max_temp, wl_start, n, wl_step,
+                                                    reinterpret_cast<float4*>(dev_out), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "blackbody LUT launch");
+    return KT_OK;
+}
+
+kt_status kt_generate_disk_lut_device(const kt_kerr_params* p, float disk_outer, uint32_t size, float* dev_out,
+                                      void* stream) {
+    if (!p || !dev_out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (size < 2) return fail(KT_ERR_INVALID_ARG, "disk temperature LUT size must be at least 2");
+    if (!std::isfinite(disk_outer) || !std::isfinite(p->disk_inner) || disk_outer <= p->disk_inner)
+        return fail(KT_ERR_INVALID_ARG, "disk radii must be finite with outer > inner: outer=%g, inner=%g",
+                    disk_outer, p->disk_inner);
+    const cudaError_t e = ktd::launch_disk_lut(size, p->a_norm, p->inv_m, p->disk_inner, disk_outer, dev_out,
+                                               (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "disk LUT launch");
+    return KT_OK;
+}
+
 kt_status kt_generate_disk_lut(const kt_kerr_params* p, float disk_outer, uint32_t size, float* out) {
     if (!p || !out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
     if (size < 2) return fail(KT_ERR_INVALID_ARG, "disk temperature LUT size must be at least 2");

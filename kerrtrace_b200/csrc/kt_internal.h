@@ -73,6 +73,12 @@ cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t*
 // FP32 FMA throughput probe: `blocks` x 512 threads, each running 8 independent FMA chains of
 // `iters` steps (16 * iters flops per thread).
 cudaError_t launch_fma_probe(int blocks, int iters, float* sink, cudaStream_t st);
+// Lookup tables on the device (kt_luts.cu): n_lambda wavelengths from wl_start in steps of
+// wl_step; disk radii from r_in to r_out.
+cudaError_t launch_blackbody_lut(uint32_t size, float max_temp, float wl_start, int n_lambda, float wl_step,
+                                 float4* out, cudaStream_t st);
+cudaError_t launch_disk_lut(uint32_t size, float a_norm, float inv_m, float r_in, float r_out, float* out,
+                            cudaStream_t st);
 
 }  // namespace ktd
 
