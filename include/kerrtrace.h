@@ -77,9 +77,9 @@ typedef struct kt_tuning {
     int32_t schedule;      /* KT_SCHED_PLAIN or KT_SCHED_WAVEFRONT */
     int32_t block_x;       /* plain: block shape, 0 = the config's block_dim */
     int32_t block_y;
-    int32_t blocks_per_sm; /* wavefront: resident blocks of 128 threads per SM, 3..6; plain (FP32 and
-                              mixed, blocks of at most 128 threads): 5 or 6 asks for that many
-                              resident blocks, anything else for the default shape */
+    int32_t blocks_per_sm; /* wavefront: resident blocks of 128 threads per SM, 3..6; plain (blocks
+                              of at most 128 threads): 5 or 6 (FP32, mixed) or 3 or 4 (FP64) asks
+                              for that many resident blocks, anything else for the default shape */
     int32_t refill_min;    /* wavefront: idle lanes a warp collects before refilling them, 1..32 */
     int32_t order;         /* kt_order; KT_ORDER_LONG_FIRST allocates a 4-byte-per-pixel buffer */
 } kt_tuning;

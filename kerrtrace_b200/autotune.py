@@ -34,9 +34,9 @@ def candidates(precision: int = 0, mode: int = 0) -> list[dict]:
     for order in (ORDER_TILES, ORDER_LONG_FIRST):
         out += [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=4, refill_min=1, order=order)
                 for bx, by in PLAIN_BLOCKS]
-        if precision != 2:  # 128-thread blocks with 5 or 6 resident per SM (FP32 and mixed)
-            out += [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=b, refill_min=1, order=order)
-                    for bx, by in PLAIN_BLOCKS_128 for b in (5, 6)]
+        # 128-thread blocks with more resident per SM: 5 or 6 (FP32 and mixed), 3 or 4 (FP64)
+        out += [dict(schedule=SCHED_PLAIN, block_x=bx, block_y=by, blocks_per_sm=b, refill_min=1, order=order)
+                for bx, by in PLAIN_BLOCKS_128 for b in ((3, 4) if precision == 2 else (5, 6))]
         # only the FP32 reference-semantics kernel has the 3/5/6 blocks-per-SM variants
         bps = WAVE_BLOCKS_PER_SM if (precision == 0 and mode == 0) else [4]
         out += [dict(schedule=SCHED_WAVEFRONT, block_x=0, block_y=0, blocks_per_sm=b, refill_min=r, order=order)

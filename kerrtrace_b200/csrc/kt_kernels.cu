@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(256) rank_pixels_kernel(const Scene sc, const 
 // Resident 256-thread blocks per SM asked of the compiler for the plain kernel: two for the
 // FP32 and mixed paths (at most 128 registers per thread, 16 warps per SM), one for FP64.
 // Blocks of at most 128 threads can also ask for 5 or 6 resident blocks (at most 102 or 85
-// registers: 20 or 24 warps per SM), a choice of the tuning (blocks_per_sm) for FP32 and mixed.
+// registers: 20 or 24 warps per SM), a choice of the tuning (blocks_per_sm) for FP32 and mixed,
+// and FP64 for 3 or 4 (at most 170 or 128 registers: 12 or 16 warps per SM instead of 8).
 template <class R> struct PlainMinBlocks { static constexpr int v = 2; };
 template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
 
@@ -335,7 +336,16 @@ static cudaError_t launch_plain(const Scene& sc, const Camera& cam, float4* hdr,
     const unsigned n = (unsigned)sc.width * (unsigned)sc.height, per = (unsigned)(bx * by);
     const dim3 grid = order ? dim3((n + per - 1) / per)
                             : dim3((sc.width + bx - 1) / bx, (sc.height + by - 1) / by);
-    if constexpr (!std::is_same<R, double>::value) {
+    if constexpr (std::is_same<R, double>::value) {
+        if (bx * by <= 128 && minb == 3) {
+            trace_plain_kernel<R, MODE, COUNT, 128, 3><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
+            return cudaGetLastError();
+        }
+        if (bx * by <= 128 && minb == 4) {
+            trace_plain_kernel<R, MODE, COUNT, 128, 4><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
+            return cudaGetLastError();
+        }
+    } else {
         if (bx * by <= 128 && minb == 5) {
             trace_plain_kernel<R, MODE, COUNT, 128, 5><<<grid, block, 0, st>>>(sc, cam, hdr, err, ctr, aux, order);
             return cudaGetLastError();
