@@ -384,8 +384,10 @@ __device__ __forceinline__ R rk_a(int m, int j) {
 }
 
 // ---- forward: record / replay ----------------------------------------------------------------
+// Four resident 128-thread blocks per SM: 128 registers at most (the FP64 kernel spills about
+// 400 B there; 192 registers and two blocks otherwise).
 template <class R, bool REPLAY>
-__global__ void __launch_bounds__(128) diff_forward_kernel(const Scene sc, const Camera cam, const CameraD camd,
+__global__ void __launch_bounds__(128, 4) diff_forward_kernel(const Scene sc, const Camera cam, const CameraD camd,
                                                           const DiffRecRaw rec, float4* __restrict__ hdr,
                                                           double* __restrict__ hdr64, uint32_t* __restrict__ err,
                                                           uint32_t* __restrict__ flags) {

@@ -188,7 +188,8 @@ __global__ void __launch_bounds__(256) rank_pixels_kernel(const Scene sc, const 
 // FP32 and mixed paths (at most 128 registers per thread, 16 warps per SM), one for FP64.
 // Blocks of at most 128 threads can also ask for 5 or 6 resident blocks (at most 102 or 85
 // registers: 20 or 24 warps per SM), a choice of the tuning (blocks_per_sm) for FP32 and mixed,
-// and FP64 for 3 or 4 (at most 170 or 128 registers: 12 or 16 warps per SM instead of 8).
+// and FP64 for 3 or 4 (at most 170 or 128 registers, with some spills: 12 or 16 warps per SM
+// instead of 8).
 template <class R> struct PlainMinBlocks { static constexpr int v = 2; };
 template <> struct PlainMinBlocks<double> { static constexpr int v = 1; };
 
