@@ -729,80 +729,6 @@ __global__ void __launch_bounds__(kVThreads) post_v_kernel(const PostParams pp,
     }
 }
 
-// Vertical pass with the bloom column tile staged in shared memory: the block loads its 64
-// columns x (32 + 2R) rows of the bloom buffer with coalesced, independent loads (the whole tile
-// in flight at once instead of each thread's column one value at a time), then makes the same
-// outputs as post_v_kernel from shared memory, in the same tap order (bit-identical).  Used
-// while the tile fits (R <= kVStagedMaxR).
-constexpr int kVStagedMaxR = 64;
-
-__global__ void __launch_bounds__(kVThreads) post_v_staged_kernel(const PostParams pp,
-                                                                   const float4* __restrict__ hdr,
-                                                                   const float4* __restrict__ bloom,
-                                                                   uint32_t* __restrict__ image) {
-    extern __shared__ float4 smv[];
-    const int R = pp.radius;
-    const int rows = kVRows + 2 * R;
-    float4* tile = smv;                                          // rows x kVCols
-    float* w = reinterpret_cast<float*>(tile + rows * kVCols);   // 2R + 2
-    float* wsum = w + 2 * R + 2;                                 // kVRows
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * kVCols, y0 = blockIdx.y * kVRows;
-    load_weights(w, R, pp.sigma, tid, blockDim.x);
-    const int total = rows * kVCols;
-    for (int j0 = tid; j0 < total; j0 += 4 * kVThreads) {  // 4 loads in flight per thread
-        float4 v[4];
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int j = j0 + b * kVThreads;
-            const int r = j / kVCols, c = j - r * kVCols;
-            const int gy = y0 - R + r, gx = x0 + c;
-            v[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (j < total && gy >= 0 && gy < pp.height && gx < pp.width) v[b] = __ldg(bloom + (size_t)gy * pp.width + gx);
-        }
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int j = j0 + b * kVThreads;
-            if (j < total) tile[j] = v[b];
-        }
-    }
-    __syncthreads();
-    if (tid < kVRows) wsum[tid] = weight_sum(y0 + tid, pp.height, w, R);
-    __syncthreads();
-    const int lane = tid & 31, warp = tid >> 5;
-    const int xc = (warp & 1) * 32 + lane;
-    const int x = x0 + xc;
-    const int rb = (warp >> 1) * kBJ;
-    const int yb = y0 + rb;
-    if (x >= pp.width || yb >= pp.height) return;
-    float acc[kBJ][3];
-    const float4* col = tile + rb * kVCols + xc;  // tile row rb + k holds image row yb - R + k
-    auto load = [col](int k) { return col[k * kVCols]; };
-    if (2 * R >= kBJ - 1 && yb - R >= 0 && yb + kBJ - 1 + R < pp.height)
-        blur_interior(load, w, R, acc);
-    else
-        blur_edge(load, w, R, yb, pp.height, acc);
-#pragma unroll
-    for (int j = 0; j < kBJ; ++j) {
-        const int y = yb + j;
-        if (y >= pp.height) break;
-        const size_t idx = (size_t)y * pp.width + x;
-        const float4 base = __ldg(hdr + idx);
-        float fr = base.x, fg = base.y, fb = base.z;
-        const float ws = wsum[rb + j];
-        float ax = acc[j][0], ay = acc[j][1], az = acc[j][2];
-        if (ws > 0.0f) {
-            ax /= ws;
-            ay /= ws;
-            az /= ws;
-        }
-        fr += ax * pp.intensity;
-        fg += ay * pp.intensity;
-        fb += az * pp.intensity;
-        image[idx] = tone_pack(fr, fg, fb);
-    }
-}
-
 // Tone map only (bloom inactive): one thread per pixel.
 __global__ void tonemap_kernel(const PostParams pp, const float4* __restrict__ hdr,
                                uint32_t* __restrict__ image) {
@@ -818,9 +744,6 @@ static size_t bloom_h_smem(int R) {
     return (size_t)kHRows * bloom_h_stride(R) * sizeof(float4) + (size_t)(2 * R + 2 + kHCols) * sizeof(float);
 }
 static size_t post_v_smem(int R) { return (size_t)(2 * R + 2 + kVRows) * sizeof(float); }
-static size_t post_v_staged_smem(int R) {
-    return (size_t)(kVRows + 2 * R) * kVCols * sizeof(float4) + (size_t)(2 * R + 2 + kVRows) * sizeof(float);
-}
 constexpr size_t kSmemLimit = 200 * 1024;
 
 static cudaError_t set_smem(const void* fn, size_t bytes) {
@@ -842,14 +765,6 @@ cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, flo
 cudaError_t launch_post_process(const PostParams& pp, const float4* hdr, const float4* bloom,
                                 uint32_t* image, cudaStream_t st) {
     if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
-    if (pp.active && pp.radius <= kVStagedMaxR) {
-        const size_t sms = post_v_staged_smem(pp.radius);
-        cudaError_t e = set_smem((const void*)post_v_staged_kernel, sms);
-        if (e != cudaSuccess) return e;
-        const dim3 grid((pp.width + kVCols - 1) / kVCols, (pp.height + kVRows - 1) / kVRows);
-        post_v_staged_kernel<<<grid, kVThreads, sms, st>>>(pp, hdr, bloom, image);
-        return cudaGetLastError();
-    }
     const size_t sm = pp.active ? post_v_smem(pp.radius) : 0;
     if (sm > kSmemLimit) return cudaErrorInvalidValue;
     cudaError_t e = set_smem((const void*)post_v_kernel, sm);
