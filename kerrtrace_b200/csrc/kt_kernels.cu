@@ -534,7 +534,7 @@ __device__ __forceinline__ void blur_interior(const Load& load, const float* w, 
     float wr[kBJ];
 #pragma unroll
     for (int j = 0; j < kBJ; ++j) wr[j] = w[kBJ - 1 - j];
-#pragma unroll 4
+#pragma unroll 8
     for (int k = kBJ - 1; k <= 2 * R; ++k) {
         const float4 v = load(k);
 #pragma unroll
