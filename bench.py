@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"],
                     help="arithmetic of the main loop (mixed / fp64 need --mode spec)")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--no-retirement", action="store_true",
+                    help="skip the leg that times the frame with NaN-frozen rays kept to max_steps")
     ap.add_argument("--no-c3", action="store_true", help="skip the 4096^2 x 8-draw precision ablation")
     ap.add_argument("--no-sequence", action="store_true", help="skip the headless frame-sequence leg")
     ap.add_argument("--no-batch", action="store_true")
@@ -167,8 +169,11 @@ def job_mrays_s(rays_per_rank: int, world: int, max_ms: float) -> float:
     return rays_per_rank * world / (max_ms / 1e3) / 1e6
 
 
-def rank_camera(kt, workloads, name, rank, world, size=None):
-    cfg, cam = workloads.scene(name)
+def rank_camera(workloads, name, rank, world, size=None, host=None):
+    """The scene of this rank: the named workload (optionally at another resolution) seen from
+    azimuth 360 * rank / world.  `host` supplies the scene's host arithmetic (the library's, or
+    the oracle's restatement in the reference arm)."""
+    cfg, cam = workloads.scene(name, host=host)
     if size:
         w, h = (int(v) for v in size.lower().split("x"))
         cfg = workloads.scaled(cfg, w, h)
@@ -176,8 +181,14 @@ def rank_camera(kt, workloads, name, rank, world, size=None):
         r = math.sqrt(sum(c * c for c in cam.cam_pos))
         incl = math.degrees(math.acos(cam.cam_pos[1] / r))
         fov = 2 * math.degrees(math.atan(cam.fov_scale))
-        cam = kt.orbit_camera(r, incl, fov, azimuth_deg=360.0 * rank / world)
+        cam = workloads.orbit_camera(r, incl, fov, azimuth_deg=360.0 * rank / world, host=host)
     return cfg, cam
+
+
+def workload_label(name: str, cfg) -> str:
+    """config.workload of both arms: the scene and the values that size its work."""
+    return (f"{name}: {cfg.width}x{cfg.height}, a={cfg.spin:.3f}, tol={cfg.tolerance:g}, "
+            f"max_steps={cfg.max_steps}, spp={cfg.spp}, bloom r={cfg.bloom_radius:g}")
 
 
 def cpu_baseline(cfg, cam, budget_s: float) -> dict:
@@ -211,6 +222,59 @@ def cpu_baseline(cfg, cam, budget_s: float) -> dict:
         rays = len(pix) * cfg.spp
         sample = f"f64 oracle, every {stride}th pixel of the {cfg.width}x{cfg.height} frame ({len(pix)} pixels) in {t:.2f} s"
     return {"value": round(rays / t / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample}
+
+
+def retirement_leg(ctx, cfg, cam, stream, reps: int = 2) -> dict:
+    """The same frame with retirement of NaN-frozen rays switched off (tuning keep_frozen = 1):
+    frozen rays then iterate to max_steps as the reference's do (cuda/kerr_trace.cuh:62,83-125),
+    so the trace does the reference's amount of work with this library's kernel.  Event-timed
+    trace of both settings on the tuned launch shape and on the default persistent shape (the
+    faster of the two is reported), the bit-identity of the two images and the work counters."""
+    import torch
+
+    import kerrtrace_b200 as kt
+    n = cfg.width * cfg.height
+    a = torch.zeros((n, 4), device="cuda")
+    b = torch.zeros((n, 4), device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    tuned = ctx.tuning().as_dict()
+    shapes = {"tuned": tuned, "wavefront_default": dict(schedule=kt.SCHED_WAVEFRONT, block_x=0, block_y=0,
+                                                        blocks_per_sm=4, refill_min=1, order=0)}
+
+    def timed(out, k):
+        ctx.trace(cam, out.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            ctx.trace(cam, out.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    res = {}
+    for label, shape in shapes.items():
+        shape = {k: v for k, v in shape.items() if k != "keep_frozen"}
+        ctx.set_tuning(**shape, keep_frozen=0)
+        t_retire = timed(a, max(3, reps))
+        ctx.set_tuning(**shape, keep_frozen=1)
+        t_keep = timed(b, reps)
+        res[label] = {"retire_ms": round(t_retire, 4), "keep_frozen_ms": round(t_keep, 4),
+                      "bit_identical": bool(torch.equal(a.view(torch.int32), b.view(torch.int32)))}
+    ctx.set_tuning(**{k: v for k, v in tuned.items() if k != "keep_frozen"}, keep_frozen=1)
+    st_keep = ctx.trace_counted(cam, b.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+    ctx.set_tuning(**tuned)
+    st = ctx.trace_counted(cam, a.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+    best = min(res, key=lambda k: res[k]["keep_frozen_ms"])
+    out = {"shapes": res, "keep_frozen_best": best,
+           "keep_frozen_trace_ms": res[best]["keep_frozen_ms"], "retire_trace_ms": res["tuned"]["retire_ms"],
+           "retirement_gain": round(res[best]["keep_frozen_ms"] / res["tuned"]["retire_ms"], 2),
+           "keep_frozen_mrays_s": round(n * cfg.spp / res[best]["keep_frozen_ms"] / 1e3, 3),
+           "bit_identical": all(r["bit_identical"] for r in res.values()),
+           "frozen_rays": int(st.frozen_rays),
+           "work_retire": {"steps": int(st.steps), "attempts": int(st.attempts), "rhs_evals": int(st.rhs_evals)},
+           "work_keep_frozen": {"steps": int(st_keep.steps), "attempts": int(st_keep.attempts),
+                                "rhs_evals": int(st_keep.rhs_evals)}}
+    return out
 
 
 def precision_leg(cfg, cam, local, reps: int) -> dict:
@@ -589,7 +653,7 @@ def run_ours(args, rank, world, local):
     import kerrtrace_b200 as kt
     from kerrtrace_b200 import autotune, flops, workloads
 
-    cfg, cam = rank_camera(kt, workloads, args.workload, rank, world, args.size)
+    cfg, cam = rank_camera(workloads, args.workload, rank, world, args.size)
     cfg.mode = kt.MODE_SPEC if args.mode == "spec" else kt.MODE_REF
     cfg.precision = {"fp32": kt.PREC_FP32, "mixed": kt.PREC_MIXED, "fp64": kt.PREC_FP64}[args.precision]
     sched = {"auto": kt.SCHED_AUTO, "wavefront": kt.SCHED_WAVEFRONT, "plain": kt.SCHED_PLAIN}[args.schedule]
@@ -701,8 +765,7 @@ def run_ours(args, rank, world, local):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, camera rays)",
-        "config": {"workload": f"{args.workload}: {cfg.width}x{cfg.height}, a={cfg.spin:.3f}, tol={cfg.tolerance:g}, "
-                               f"max_steps={cfg.max_steps}, spp={cfg.spp}, bloom r={cfg.bloom_radius:g}",
+        "config": {"workload": workload_label(args.workload, cfg),
                    "schedule": args.schedule, "tuning": t.as_dict(),
                    "mode": "reference semantics (drop-in, bit-identical to the reference kernel)" if args.mode == "ref"
                    else "stated physics", "precision": args.precision,
@@ -714,7 +777,8 @@ def run_ours(args, rank, world, local):
         line["autotune"] = tuned.summary()
     # legs, each with the SM clock sampled while it runs; the long 4096^2 ablation goes last, so
     # that the heat it leaves does not lower the clocks of the shorter legs
-    legs = [("precision", args.no_precision, lambda: precision_leg(cfg, cam, local, max(3, args.steps))),
+    legs = [("retirement", args.no_retirement, lambda: retirement_leg(ctx, cfg, cam, stream)),
+            ("precision", args.no_precision, lambda: precision_leg(cfg, cam, local, max(3, args.steps))),
             ("adjoint", args.no_adjoint, lambda: adjoint_leg(local, max(3, args.steps))),
             ("batch", args.no_batch, lambda: batch_leg(local, 3)),
             ("sequence", args.no_sequence, lambda: sequence_leg(cfg, ctx.tuning(), local)),
@@ -732,23 +796,24 @@ def run_ours(args, rank, world, local):
 
 
 def run_reference(args, rank, world, local):
+    """The reference's own implementation of the path: its cuda/kernel.cu, compiled from source
+    into oracle/_ref, launched like src/renderer/mod.rs:149-209.  Its scene values, KerrParams,
+    LUTs and cameras come from the oracle's restatement of the reference host, so this process
+    maps no product library."""
     import numpy as np
     import torch
 
-    import kerrtrace_b200 as kt
     import oracle
     from kerrtrace_b200 import workloads
 
     if rank != 0:
         return
-    cfg, cam = rank_camera(kt, workloads, args.workload, 0, 1, args.size)
+    host = oracle.Host()
+    cfg, cam = rank_camera(workloads, args.workload, 0, 1, args.size, host=host)
     if not oracle.ref_lib_path(args.workload).exists():
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/libktref_{args.workload}.so not built"}))
         return
-    p = kt.build_kerr_params(cfg)
-    bb = kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start, cfg.wavelength_end,
-                                   cfg.wavelength_step)
-    disk = kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)
+    p, bb, disk = oracle.reference_inputs(cfg)
     ref = oracle.RefKernel(args.workload)
     ref.setup(p, bb, disk)
     n = cfg.width * cfg.height
@@ -762,7 +827,7 @@ def run_reference(args, rank, world, local):
     sigma = float(np.float32(cfg.bloom_radius) / np.float32(3.0))
     active = int(bool(cfg.bloom_enabled) and radius > 0 and cfg.bloom_intensity > 0)
 
-    def frame():  # src/renderer/mod.rs:543-603
+    def frame():  # src/renderer/mod.rs:149-209
         err.zero_()
         ref.trace(hdr.data_ptr(), cfg, cam, cfg.lut_max_temp, err.data_ptr(), p.disk_inner)
         host_err.copy_(err, non_blocking=True)
@@ -792,7 +857,7 @@ def run_reference(args, rank, world, local):
             "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, camera rays)",
-            "config": {"workload": f"{args.workload}: {cfg.width}x{cfg.height}",
+            "config": {"workload": workload_label(args.workload, cfg),
                        "implementation": "reference cuda/kernel.cu compiled from source for sm_100a "
                                          "(-use_fast_math, the reference's #define header), mod.rs launch sequence"},
             "e2e": {"value": round(rays / wall / 1e6, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 52,

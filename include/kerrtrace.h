@@ -9,7 +9,7 @@
  *
  * Conventions
  *  - Every `stream` argument is a `cudaStream_t` passed as `void*` (NULL = legacy default
- *    stream, the one cudarc's `context.default_stream()` uses, src/renderer/mod.rs:474).
+ *    stream, the one cudarc's `context.default_stream()` uses, src/renderer/mod.rs:80).
  *  - Device pointers are marked `dev`; host pointers `host`.  The caller owns every output
  *    buffer.  A context owns its LUT textures and the small scratch words of the wavefront
  *    tracer; calls on one context must be ordered on one stream at a time.
@@ -30,15 +30,15 @@
 extern "C" {
 #endif
 
-#define KT_ABI_VERSION 2
+#define KT_ABI_VERSION 3
 
 typedef enum kt_status {
     KT_OK = 0,
     KT_ERR_INVALID_ARG = 1,   /* bad config / pointer / size (reference: anyhow! in utils.rs, init.rs) */
     KT_ERR_CUDA = 2,          /* a CUDA runtime call failed (reference: cudarc DriverError) */
-    KT_ERR_LUT_OVERFLOW = 3,  /* colour temperature above lut_max_temp (mod.rs:630-635) */
-    KT_ERR_NOT_READY = 4,     /* frame not complete yet (mod.rs:620 returns Ok(None)) */
-    KT_ERR_QUEUE_ORDER = 5,   /* finish_frame out of order (mod.rs:646-650) */
+    KT_ERR_LUT_OVERFLOW = 3,  /* colour temperature above lut_max_temp (mod.rs:236-241) */
+    KT_ERR_NOT_READY = 4,     /* frame not complete yet (mod.rs:226-228 returns Ok(None)) */
+    KT_ERR_QUEUE_ORDER = 5,   /* finish_frame out of order (mod.rs:253-256) */
     KT_ERR_NO_DEVICE = 6,     /* no CUDA device / library built without one */
     KT_ERR_UNSUPPORTED = 7,   /* option not available in this build */
     KT_ERR_TIMEOUT = 8        /* a bounded device wait gave up */
@@ -82,6 +82,11 @@ typedef struct kt_tuning {
                               for that many resident blocks, anything else for the default shape */
     int32_t refill_min;    /* wavefront: idle lanes a warp collects before refilling them, 1..32 */
     int32_t order;         /* kt_order; KT_ORDER_LONG_FIRST allocates a 4-byte-per-pixel buffer */
+    int32_t keep_frozen;   /* 0 (default): a ray whose state has become NaN (the reference's
+                              tolerance reaches 0 near the hole, cuda/kerr_trace.cuh:66-73) is
+                              retired at that step; 1: it iterates to max_steps like the
+                              reference's (kerr_trace.cuh:62,83-125).  Same image bits either way;
+                              1 only serves to time the reference's amount of work. */
 } kt_tuning;
 
 /*
@@ -148,7 +153,7 @@ typedef struct kt_kerr_params {
     int32_t disk_noise_enabled, disk_noise_detail;
 } kt_kerr_params;
 
-/* Camera of one frame: the arguments of CudaRenderer::submit_render (mod.rs:513-520). */
+/* Camera of one frame: the arguments of CudaRenderer::submit_render (mod.rs:119-126). */
 typedef struct kt_camera {
     float cam_pos[3];
     float fwd[3];
@@ -224,10 +229,10 @@ void kt_context_destroy(kt_context* ctx);
 /* Copies out the derived KerrParams the context uses. */
 kt_status kt_context_params(const kt_context* ctx, kt_kerr_params* out);
 
-/* ---- per-frame kernels: replace the three launches of submit_render (mod.rs:547-600) ------ */
+/* ---- per-frame kernels: replace the three launches of submit_render (mod.rs:153-206) ------ */
 /* trace_kernel (cuda/kernel.cu:88-142): writes W*H float4 (r,g,b,1) HDR, row-major.
  * hdr_out: dev float[4*W*H]; err_word: dev uint32[2] (not cleared here, like the reference,
- * which clears it with memset_zeros before the launch, mod.rs:544-546). */
+ * which clears it with memset_zeros before the launch, mod.rs:150-152). */
 kt_status kt_trace(kt_context* ctx, void* stream, const kt_camera* cam, int32_t schedule,
                    float* hdr_out, uint32_t* err_word);
 /* Same as kt_trace, plus per-launch counters (synchronises the stream to read them).
@@ -257,6 +262,27 @@ kt_status kt_trace_progressive(kt_context* ctx, void* stream, const kt_camera* c
  * context allocates the order buffer. */
 kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* tuning);
 kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* tuning);
+
+/* Launch-shape autotuner (no reference counterpart: the reference launches its trace on the
+ * config's block_dim, src/renderer/mod.rs:132-136 and init.rs compute_launch_dims).  Times the
+ * trace of `cam` under each candidate tuning with CUDA events on `stream` (one warm-up launch,
+ * then `reps` launches, 1..64, scored by the median), keeps only candidates whose image is bit
+ * for bit the first candidate's, and installs the fastest of those in the context
+ * (kt_context_set_tuning); kt_trace(KT_SCHED_AUTO) then runs it.  candidates == NULL uses the
+ * built-in list (plain block shapes, 128-thread plain blocks with more resident blocks per SM,
+ * wavefront blocks per SM x refill thresholds, each in tile and long-rays-first order; at most
+ * KT_TUNE_MAX_CANDIDATES, keep_frozen taken from the current tuning).  table (may be NULL)
+ * receives one row per candidate, *n_entries their number.  Allocates scratch for one frame
+ * and synchronises `stream`; call it at set-up, outside stream capture. */
+#define KT_TUNE_MAX_CANDIDATES 64
+typedef struct kt_tune_entry {
+    kt_tuning tuning;
+    float ms;          /* median trace time of the candidate */
+    int32_t identical; /* 1 when its image equals the first candidate's bit for bit */
+} kt_tune_entry;
+kt_status kt_context_autotune(kt_context* ctx, void* stream, const kt_camera* cam, uint32_t reps,
+                              const kt_tuning* candidates, uint32_t n_candidates, kt_tune_entry* table,
+                              uint32_t* n_entries);
 /* bloom_horizontal (cuda/kernel.cu:144-173): dev float4 hdr -> dev float4 bloom. */
 kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom);
 /* post_process (cuda/kernel.cu:175-251): vertical blur + composite + ACES + sRGB + pack to
@@ -323,19 +349,19 @@ kt_status kt_trace_noalloc(const kt_config* cfg, const kt_camera* cams, uint32_t
                            const float* bb_lut, const float* disk_lut, void* stream,
                            float* hdr_out, uint32_t* err_words);
 
-/* ---- CudaRenderer mirror (src/renderer/mod.rs:469-687) ------------------------------------ */
-/* CudaRenderer::new (mod.rs:470-511): context + two frame buffers with pinned host images. */
+/* ---- CudaRenderer mirror (src/renderer/mod.rs:52-293) ------------------------------------ */
+/* CudaRenderer::new (mod.rs:76-117): context + two frame buffers with pinned host images. */
 kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out);
-/* CudaRenderer::submit_render (mod.rs:513-612).  *submitted = 0 when both frames are in
+/* CudaRenderer::submit_render (mod.rs:119-218).  *submitted = 0 when both frames are in
  * flight (the reference returns Ok(false)). */
 kt_status kt_renderer_submit_render(kt_renderer* r, const float cam_pos[3], const float fwd[3],
                                     const float rgt[3], const float up[3], float fov_scale,
                                     int32_t* submitted);
-/* CudaRenderer::ready_frame (mod.rs:614-644).  Returns KT_ERR_NOT_READY when no frame is
+/* CudaRenderer::ready_frame (mod.rs:220-250).  Returns KT_ERR_NOT_READY when no frame is
  * complete, KT_ERR_LUT_OVERFLOW (and *overflow_temp) when the frame's error word was set. */
 kt_status kt_renderer_ready_frame(kt_renderer* r, uint32_t* index, const uint32_t** data,
                                   float* overflow_temp);
-/* CudaRenderer::finish_frame (mod.rs:646-654). */
+/* CudaRenderer::finish_frame (mod.rs:252-260). */
 kt_status kt_renderer_finish_frame(kt_renderer* r, uint32_t index);
 /* Blocks until every submitted frame is complete (no reference counterpart; used by hosts
  * that render headless). */
@@ -344,6 +370,11 @@ kt_status kt_renderer_wait(kt_renderer* r);
 kt_status kt_renderer_set_schedule(kt_renderer* r, int32_t schedule);
 /* Sets the launch shape of the renderer's context (kt_context_set_tuning). */
 kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning);
+/* Runs kt_context_autotune on the renderer's context and stream for the view `cam` (its
+ * built-in candidates); submit_render then uses the installed shape.  Synchronises; call it
+ * after kt_renderer_new and before the first frame (a Rust CudaRenderer::new, mod.rs:76-117,
+ * would call it once with the config's initial camera). */
+kt_status kt_renderer_autotune(kt_renderer* r, const kt_camera* cam, uint32_t reps);
 /* The device HDR buffer of a frame (valid until the frame is resubmitted). */
 kt_status kt_renderer_frame_hdr(kt_renderer* r, uint32_t index, const float** hdr_dev);
 void kt_renderer_destroy(kt_renderer* r);

@@ -92,10 +92,20 @@ class KtTuning(C.Structure):
     """Mirror of ``kt_tuning``: the launch shape that KT_SCHED_AUTO runs."""
 
     _fields_ = [("schedule", C.c_int32), ("block_x", C.c_int32), ("block_y", C.c_int32),
-                ("blocks_per_sm", C.c_int32), ("refill_min", C.c_int32), ("order", C.c_int32)]
+                ("blocks_per_sm", C.c_int32), ("refill_min", C.c_int32), ("order", C.c_int32),
+                ("keep_frozen", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+TUNE_MAX_CANDIDATES = 64
+
+
+class KtTuneEntry(C.Structure):
+    """Mirror of ``kt_tune_entry``: one candidate of the autotuner."""
+
+    _fields_ = [("tuning", KtTuning), ("ms", C.c_float), ("identical", C.c_int32)]
 
 
 class KtDiffParams(C.Structure):
@@ -176,6 +186,9 @@ SIGNATURES = [
     ("kt_context_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
     ("kt_context_get_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
     ("kt_renderer_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
+    ("kt_context_autotune", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_uint32, C.c_void_p,
+                                      C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),
+    ("kt_renderer_autotune", C.c_int, [C.c_void_p, C.POINTER(KtCamera), C.c_uint32]),
     ("kt_bloom_horizontal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_post_process", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_post_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -380,8 +393,10 @@ class Context:
                                          C.c_void_p(accum_ptr), C.c_void_p(hdr_ptr), C.c_void_p(err_ptr)))
 
     def set_tuning(self, schedule: int = SCHED_WAVEFRONT, block_x: int = 0, block_y: int = 0,
-                   blocks_per_sm: int = 4, refill_min: int = 1, order: int = 0):
-        t = KtTuning(schedule, block_x, block_y, blocks_per_sm, refill_min, order)
+                   blocks_per_sm: int = 4, refill_min: int = 1, order: int = 0, keep_frozen: int = 0):
+        """keep_frozen=1 lets NaN-frozen rays iterate to max_steps as the reference's do (same
+        image; for timing the reference's amount of work)."""
+        t = KtTuning(schedule, block_x, block_y, blocks_per_sm, refill_min, order, keep_frozen)
         check(lib().kt_context_set_tuning(self.handle, C.byref(t)))
 
     def tuning(self) -> KtTuning:
@@ -515,7 +530,7 @@ class LutOverflow(KtError):
 
 
 class Renderer:
-    """Mirror of the reference's CudaRenderer (src/renderer/mod.rs:469-687)."""
+    """Mirror of the reference's CudaRenderer (src/renderer/mod.rs:52-293)."""
 
     def __init__(self, cfg: KtConfig, device: int = 0):
         self.cfg = cfg.copy()
@@ -528,6 +543,10 @@ class Renderer:
 
     def set_tuning(self, tuning: KtTuning):
         check(lib().kt_renderer_set_tuning(self.handle, C.byref(tuning)))
+
+    def autotune(self, cam: KtCamera, reps: int = 3):
+        """kt_renderer_autotune: tunes the launch shape of submit_render for the view `cam`."""
+        check(lib().kt_renderer_autotune(self.handle, C.byref(cam), reps))
 
     def submit_render(self, cam_pos, fwd, rgt, up, fov_scale: float) -> bool:
         arr = lambda v: (C.c_float * 3)(*v)  # noqa: E731

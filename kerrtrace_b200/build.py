@@ -80,12 +80,15 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     dh_obj = BUILD / "kt_diff_host.o"
     _run([gxx, "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", *inc,
           "-I", str(cuda_home / "include"), "-c", str(CSRC / "kt_diff_host.cpp"), "-o", str(dh_obj)])
+    t_obj = BUILD / "kt_tune.o"
+    _run([gxx, "-std=c++17", "-O2", "-fPIC", *inc, "-I", str(cuda_home / "include"), "-c", str(CSRC / "kt_tune.cpp"),
+          "-o", str(t_obj)])
     a_obj = BUILD / "kt_app.o"
     _run([gxx, "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", *inc,
           "-I", str(cuda_home / "include"), "-c", str(CSRC / "kt_app.cpp"), "-o", str(a_obj)])
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-cudart", "static", str(k_obj), str(n_obj), str(d_obj), str(h_obj), str(dh_obj),
-          str(a_obj), str(l_obj), "-o", str(tmp)])
+          str(a_obj), str(l_obj), str(t_obj), "-o", str(tmp)])
     os.replace(tmp, LIB)
     return LIB
 

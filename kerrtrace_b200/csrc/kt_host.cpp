@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/kerrtrace.h"
+#include "kt_context.h"
 #include "kt_internal.h"
 
 namespace {
@@ -449,23 +450,7 @@ kt_status kt_validate_bloom(const kt_config* cfg, int32_t* enabled, float* inten
 // =========================================================================================
 // Device context
 // =========================================================================================
-struct kt_context {
-    int device = 0;
-    kt_config cfg{};
-    kt_kerr_params params{};
-    ktd::Scene scene{};
-    ktd::PostParams post{};
-    cudaArray_t bb_array = nullptr, disk_array = nullptr;
-    cudaTextureObject_t bb_tex = 0, disk_tex = 0;
-    float4* bb_lut_dev = nullptr;
-    float* disk_lut_dev = nullptr;
-    unsigned* queue = nullptr;              // wavefront work counter (1 word)
-    ktd::Tuning tuning;                     // persistent-tracer launch shape
-    unsigned long long* counters = nullptr; // 6 x u64 for the counting launches
-    unsigned* order = nullptr;              // pixel order (allocated when a tuning asks for it)
-    float4* bloom_scratch = nullptr;        // kt_post_fused's bloom buffer (when bloom is active)
-    int block_x = 16, block_y = 16;
-};
+// struct kt_context is defined in kt_context.h (shared with the autotuner, kt_tune.cpp).
 
 namespace {
 
@@ -761,6 +746,8 @@ kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* t) {
         return fail(KT_ERR_INVALID_ARG, "plain block %dx%d invalid", t->block_x, t->block_y);
     if (t->order != KT_ORDER_TILES && t->order != KT_ORDER_LONG_FIRST)
         return fail(KT_ERR_INVALID_ARG, "tuning order %d must be tiles or long-first", t->order);
+    if (t->keep_frozen != 0 && t->keep_frozen != 1)
+        return fail(KT_ERR_INVALID_ARG, "tuning keep_frozen %d must be 0 or 1", t->keep_frozen);
     if (t->order == KT_ORDER_LONG_FIRST && !ctx->order) {
         DeviceGuard g(ctx->device);
         const size_t words = ktd::kOrderHeader + (size_t)ctx->cfg.width * ctx->cfg.height;
@@ -772,6 +759,8 @@ kt_status kt_context_set_tuning(kt_context* ctx, const kt_tuning* t) {
     ctx->tuning.block_y = t->block_y;
     ctx->tuning.blocks_per_sm = t->blocks_per_sm;
     ctx->tuning.refill_min = t->refill_min;
+    ctx->tuning.keep_frozen = t->keep_frozen;
+    ctx->scene.keep_frozen = t->keep_frozen;
     return KT_OK;
 }
 kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* t) {
@@ -782,6 +771,7 @@ kt_status kt_context_get_tuning(const kt_context* ctx, kt_tuning* t) {
     t->blocks_per_sm = ctx->tuning.blocks_per_sm;
     t->refill_min = ctx->tuning.refill_min;
     t->order = ctx->tuning.order;
+    t->keep_frozen = ctx->tuning.keep_frozen;
     return KT_OK;
 }
 
@@ -1028,6 +1018,10 @@ kt_status kt_renderer_set_schedule(kt_renderer* r, int32_t schedule) {
     return KT_OK;
 }
 
+kt_status kt_renderer_autotune(kt_renderer* r, const kt_camera* cam, uint32_t reps) {
+    if (!r || !cam) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    return kt_context_autotune(r->ctx, r->stream, cam, reps, nullptr, 0, nullptr, nullptr);
+}
 kt_status kt_renderer_set_tuning(kt_renderer* r, const kt_tuning* tuning) {
     if (!r) return fail(KT_ERR_INVALID_ARG, "renderer is NULL");
     return kt_context_set_tuning(r->ctx, tuning);

@@ -8,7 +8,7 @@
 
 namespace ktd {
 
-// Bloom / post-process constants of one context (src/renderer/init.rs:43-73, mod.rs:533-542).
+// Bloom / post-process constants of one context (src/renderer/init.rs:43-73, mod.rs:139-148).
 struct PostParams {
     int width, height;
     int radius;       // ceil(bloom.radius)
@@ -28,6 +28,7 @@ struct Tuning {
     int blocks_per_sm = 4;
     int refill_min = 1;
     int order = 0;  // 1: pixels ranked long-rays-first by the rank kernel before the trace
+    int keep_frozen = 0;  // 1: NaN-frozen rays iterate to max_steps (Scene::keep_frozen)
 };
 
 // Pixel-order buffer: kOrderHeader header words (marked / unmarked counts), then one pixel
@@ -62,6 +63,9 @@ struct BatchTable {
     int total_tiles;
 };
 cudaError_t launch_batch(const BatchTable& bt, int bx, int by, cudaStream_t stream);
+// Number of 16-byte words that differ between a and b (n16 words each) into *out (device).
+cudaError_t launch_count_mismatch(const void* a, const void* b, size_t n16, unsigned long long* out,
+                                  cudaStream_t stream);
 
 cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, float4* bloom,
                                     cudaStream_t stream);

@@ -467,6 +467,31 @@ cudaError_t launch_batch(const BatchTable& bt, int bx, int by, cudaStream_t st) 
     return launch_batch_typed<float, 0>(bt, bx, by, st);
 }
 
+// ---- image comparison (the autotuner's bit-identity filter) ---------------------------------
+__global__ void __launch_bounds__(256) count_mismatch_kernel(const uint4* __restrict__ a, const uint4* __restrict__ b,
+                                                             size_t n, unsigned long long* __restrict__ out) {
+    unsigned long long local = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint4 x = __ldg(a + i), y = __ldg(b + i);
+        local += (x.x != y.x || x.y != y.y || x.z != y.z || x.w != y.w) ? 1u : 0u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(kFull, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
+cudaError_t launch_count_mismatch(const void* a, const void* b, size_t n16, unsigned long long* out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess || n16 == 0) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const size_t want = (n16 + 255) / 256;
+    const unsigned blocks = (unsigned)(want < (size_t)sms * 8 ? want : (size_t)sms * 8);
+    count_mismatch_kernel<<<blocks, 256, 0, st>>>(static_cast<const uint4*>(a), static_cast<const uint4*>(b), n16, out);
+    return cudaGetLastError();
+}
+
 // =========================================================================================
 // Post-processing
 // =========================================================================================

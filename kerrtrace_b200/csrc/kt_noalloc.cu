@@ -61,7 +61,8 @@ __device__ __forceinline__ void noalloc_unit_to_pixel(unsigned u, int W, int H, 
 // counter of its current view and moves to the next view when that counter is exhausted;
 // every lane remembers the view of the pixel it holds.
 __global__ void __launch_bounds__(kNoallocBlock, 4)
-    trace_views_noalloc_kernel(const Scene sc, const NoallocViews views, float4* __restrict__ hdr,
+    trace_views_noalloc_kernel(const __grid_constant__ Scene sc, const __grid_constant__ NoallocViews views,
+                               float4* __restrict__ hdr,
                                uint32_t* __restrict__ err, unsigned* __restrict__ queue) {
     constexpr int MODE = 2;
     const int lane = threadIdx.x & 31;
@@ -112,7 +113,13 @@ __global__ void __launch_bounds__(kNoallocBlock, 4)
                 }
             }
         }
-        if (!__any_sync(kFullMask, active)) break;
+        // A warp with no ray in flight goes back for more pixels while views remain: a claim
+        // can come back empty (its view was used up, or every claimed pixel had no ray work,
+        // e.g. max_steps = 0), and `view` has then already moved on to the next view.
+        if (!__any_sync(kFullMask, active)) {
+            if (!open) break;
+            continue;
+        }
         if (active && ray_advance<float, MODE, false>(ry, sc, err + 2 * lview, tl)) {
             acc[0] += ry.col[0];
             acc[1] += ry.col[1];

@@ -14,7 +14,8 @@
 // Arithmetic follows the reference expression by expression; the only behavioural addition is
 // retirement of rays whose state has become NaN (see ray_advance), which cannot change the
 // output: once y is NaN every later crossing / horizon / escape comparison is false and the
-// reference keeps iterating without touching the colour until max_steps.
+// reference keeps iterating without touching the colour until max_steps.  Scene::keep_frozen
+// turns retirement off, so that the reference's schedule of work can be timed as well.
 #pragma once
 #include "kt_device.cuh"
 
@@ -391,7 +392,7 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     if (COUNT) tl.steps++;
     if (O::isnanr(ry.s[1])) {  // frozen: no later comparison can succeed (see file comment)
         if (COUNT) tl.frozen = 1;
-        return true;
+        if (!sc.keep_frozen) return true;
     }
     const R r_now = ks_radius<R>(ry.s[0], ry.s[1], ry.s[2], aa);
     if (inside_horizon<R>(r_now, sc)) return true;
@@ -667,7 +668,7 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
     if (COUNT) tl.steps++;
     if (O::isnanr(ry.s[1])) {
         if (COUNT) tl.frozen = 1;
-        return true;
+        if (!sc.keep_frozen) return true;
     }
     const float r_now = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa);
     if (inside_horizon<float>(r_now, sc)) return true;

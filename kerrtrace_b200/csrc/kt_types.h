@@ -59,6 +59,10 @@ struct Scene {
     int sample_first;
     int pixel_centre;
     float4* accum;
+    // 1: a ray whose state has become NaN keeps iterating to max_steps, as the reference's
+    // does (cuda/kerr_trace.cuh:62,83-125); 0 (default): it is retired at that commit.  The
+    // image is the same either way; the switch measures what retirement saves.
+    int keep_frozen;
 };
 
 struct Camera {

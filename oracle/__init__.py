@@ -70,6 +70,10 @@ def olib() -> C.CDLL:
         L.kto_blackbody_lut.argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
         L.kto_disk_lut.argtypes = [C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_void_p]
         L.kto_params.argtypes = [C.POINTER(KtoScene), C.c_void_p]
+        L.kto_camera_basis.argtypes = [C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.kto_camera_basis.restype = None
+        L.kto_fov_scale.argtypes = [C.c_float]
+        L.kto_fov_scale.restype = C.c_float
         L.kto_isco.argtypes = [C.c_float, C.c_int, C.c_float]
         L.kto_isco.restype = C.c_float
         L.kto_nt_factor.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float]
@@ -116,6 +120,118 @@ def disk_lut(spin, mass, disk_outer, size) -> np.ndarray:
     if olib().kto_disk_lut(spin, mass, disk_outer, size, out.ctypes.data) != 0:
         raise ValueError("invalid disk LUT arguments")
     return out
+
+
+# ---- the reference host's set-up values, restated ------------------------------------------
+# The reference derives its kernel inputs on the host (src/renderer/utils.rs, blackbody.rs,
+# src/math.rs, src/app.rs).  These functions give those values from the oracle's own
+# restatement, so that a run of the reference kernel (RefKernel) takes none of its inputs from
+# the product library.
+
+# config.yaml:1-67, the fields the kernel path reads (window size, renderer block, bloom,
+# blackbody LUT, cuda, kernel, disk_noise); the YAML's max_steps 1e2 is the integer 100.
+CONFIG_YAML = {
+    "width": 2100, "height": 900, "block_dim": (16, 16),
+    "bloom_enabled": 1, "bloom_intensity": 0.5, "bloom_radius": 48.0,
+    "lut_size": 4096, "lut_max_temp": 3e4, "wavelength_start": 380.0, "wavelength_end": 720.0,
+    "wavelength_step": 10.0, "use_fast_math": 1,
+    "spp": 4, "exposure_scale": 3e-3, "sky_grid_divisions": 40, "sky_line_thickness": 5e-4, "sky_intensity": 30.0,
+    "spin": -0.45, "mass": 0.5, "disk_outer_radius": 40.0, "disk_temperature_scale": 3e4,
+    "initial_step": 1.0, "tolerance": 1e-5, "max_steps": 100, "max_attempts": 3, "transmittance_cutoff": 1e-2,
+    "horizon_epsilon": 5e-7, "escape_radius": 80.0,
+    "noise_enabled": 1, "noise_scale": 0.1, "noise_strength": 0.6, "noise_winding": 50.0, "noise_detail": 10,
+}
+
+
+class KtoKerrParams(C.Structure):
+    """The reference's KerrParams (src/renderer/init.rs:15-33, cuda/kerr_math.cuh:3-9)."""
+
+    _fields_ = [(n, C.c_float) for n in ("a", "m", "aa", "inv_m", "a_norm", "rh", "disk_inner",
+                                         "inv_w_2", "inv_h_2", "aspect_ratio", "disk_noise_scale",
+                                         "disk_noise_strength", "disk_noise_winding")] + [
+        ("disk_noise_enabled", C.c_int32), ("disk_noise_detail", C.c_int32)]
+
+
+def config_default(cfg_type):
+    """A `cfg_type` structure (any ctypes structure with the config field names) holding
+    config.yaml's values; fields config.yaml does not have stay zero, except the stated-physics
+    extension `photon_zone_factor`, whose default is 1.5."""
+    c = cfg_type()
+    names = {n for n, _ in cfg_type._fields_}
+    for k, v in CONFIG_YAML.items():
+        if k == "block_dim":
+            c.block_dim[0], c.block_dim[1] = v
+        else:
+            setattr(c, k, v)
+    if "photon_zone_factor" in names:
+        c.photon_zone_factor = 1.5
+    return c
+
+
+def _scene_of(cfg) -> "KtoScene":
+    s = KtoScene()
+    for name, _ in KtoScene._fields_:
+        if name in ("bb_lut", "disk_lut", "mode", "tex_mode", "retire_frozen", "cam_pos", "fwd", "rgt", "up",
+                    "fov_scale", "noise_seed", "noise_phase"):
+            continue
+        setattr(s, name, getattr(cfg, name))
+    return s
+
+
+def kerr_params(cfg) -> KtoKerrParams:
+    """build_kerr_params (src/renderer/utils.rs:53-113) from the oracle's restatement."""
+    v = np.zeros(10, np.float32)
+    if olib().kto_params(C.byref(_scene_of(cfg)), v.ctypes.data) != 0:
+        raise ValueError("invalid scene for the Kerr parameters")
+    return KtoKerrParams(*[float(x) for x in v], float(cfg.noise_scale), float(cfg.noise_strength),
+                         float(cfg.noise_winding), 1 if cfg.noise_enabled else 0, int(cfg.noise_detail))
+
+
+def camera_basis(yaw_deg: float, pitch_deg: float):
+    """calculate_camera_basis (src/math.rs:3-14): (forward, right, up)."""
+    f, r, u = (C.c_float * 3)(), (C.c_float * 3)(), (C.c_float * 3)()
+    olib().kto_camera_basis(yaw_deg, pitch_deg, f, r, u)
+    return list(f), list(r), list(u)
+
+
+def fov_scale(fov_deg: float) -> float:
+    """tan(fov.to_radians() / 2) (src/app.rs:163)."""
+    return float(olib().kto_fov_scale(fov_deg))
+
+
+class Host:
+    """The host arithmetic a named scene needs (config defaults, the horizon radius, the disk
+    table's peak, the camera basis), taken from the oracle's restatement.  Passed to the scene
+    builders of kerrtrace_b200.workloads by the runs of the reference kernel, so that those runs
+    map no product library."""
+
+    def config_default(self):
+        from kerrtrace_b200 import KtConfig  # the structure layout only; no library is loaded
+        return config_default(KtConfig)
+
+    def horizon_radius(self, cfg) -> float:
+        return float(kerr_params(cfg).rh)
+
+    def disk_lut(self, cfg) -> np.ndarray:
+        return disk_lut(cfg.spin, cfg.mass, cfg.disk_outer_radius, cfg.lut_size)
+
+    def camera(self, pos, yaw_deg: float, pitch_deg: float, fov_deg: float):
+        from kerrtrace_b200 import KtCamera
+        f, r, u = camera_basis(yaw_deg, pitch_deg)
+        cam = KtCamera()
+        for i in range(3):
+            cam.cam_pos[i], cam.fwd[i], cam.rgt[i], cam.up[i] = pos[i], f[i], r[i], u[i]
+        cam.fov_scale = fov_scale(fov_deg)
+        return cam
+
+
+def reference_inputs(cfg):
+    """(KerrParams, blackbody LUT, disk LUT) as the reference host builds them for `cfg`, from
+    the oracle's restatement (utils.rs:53-113, blackbody.rs:56-124, utils.rs:172-201)."""
+    p = kerr_params(cfg)
+    bb = blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start, cfg.wavelength_end, cfg.wavelength_step)
+    dk = disk_lut(cfg.spin, cfg.mass, cfg.disk_outer_radius, cfg.lut_size)
+    return p, bb, dk
 
 
 class Scene:

@@ -9,7 +9,7 @@
 
 The `#define` text is produced here independently of the product library, with Rust's
 `{:.10}` formatting of the f32 value (Python's exact decimal formatting of the same binary
-value).
+value); the scene values it formats come from the oracle's host restatement.
 """
 from __future__ import annotations
 
@@ -21,7 +21,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-REF_DIR = Path("/root/reference")
+# The reference source tree (read only); KT_REFERENCE_DIR overrides the default location.
+REF_DIR = Path(os.environ.get("KT_REFERENCE_DIR", "/root/reference"))
 REF_OUT = HERE / "_ref"
 ORACLE_LIB = HERE / "libkt_oracle.so"
 REF_SCENES = ("c1", "c2", "t1", "t2")
@@ -68,12 +69,14 @@ def build_reference(force: bool = False) -> list[Path]:
     if not (REF_DIR / "cuda" / "kernel.cu").exists():
         return []
     sys.path.insert(0, str(ROOT))
+    import oracle
     from kerrtrace_b200 import workloads
+    host = oracle.Host()  # scene values from the oracle's host restatement, not the product
     REF_OUT.mkdir(exist_ok=True)
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     built = []
     for name in REF_SCENES:
-        cfg, _ = workloads.scene(name)
+        cfg, _ = workloads.scene(name, host=host)
         hdr = REF_OUT / f"defines_{name}.h"
         text = defines_text(cfg)
         lib = REF_OUT / f"libktref_{name}.so"

@@ -1081,6 +1081,37 @@ int kto_params(const kto_scene* s, float* out10) {
     return 0;
 }
 float kto_isco(float a_norm, int prograde, float mass) { return isco(a_norm, prograde != 0, mass); }
+
+// Camera basis of the app (src/math.rs:3-14) in f32 as glam computes it: Rust's
+// f32::to_radians multiplies by the f32 constant PI / 180; Vec3::normalize scales by the
+// reciprocal of sqrt(x*x + y*y + z*z); cross products are component-wise differences of
+// products.  This file is built without FMA contraction, like Rust code.
+namespace {
+constexpr float kDegToRad = 3.14159265358979323846f / 180.0f;
+void glam_normalize(float v[3]) {
+    const float len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const float inv = 1.0f / len;
+    for (int i = 0; i < 3; ++i) v[i] = v[i] * inv;
+}
+void glam_cross(const float a[3], const float b[3], float out[3]) {
+    out[0] = a[1] * b[2] - b[1] * a[2];
+    out[1] = a[2] * b[0] - b[2] * a[0];
+    out[2] = a[0] * b[1] - b[0] * a[1];
+}
+}  // namespace
+void kto_camera_basis(float yaw_deg, float pitch_deg, float* fwd, float* rgt, float* up) {
+    const float yaw = yaw_deg * kDegToRad, pitch = pitch_deg * kDegToRad;
+    float f[3] = {std::sin(yaw) * std::cos(pitch), std::sin(pitch), -std::cos(yaw) * std::cos(pitch)};
+    glam_normalize(f);
+    const float world_up[3] = {0.0f, 1.0f, 0.0f};
+    glam_cross(f, world_up, rgt);
+    glam_normalize(rgt);
+    glam_cross(rgt, f, up);
+    glam_normalize(up);
+    for (int i = 0; i < 3; ++i) fwd[i] = f[i];
+}
+// fov_scale = (fov.to_radians() / 2.0).tan() (src/app.rs:163).
+float kto_fov_scale(float fov_deg) { return std::tan(fov_deg * kDegToRad / 2.0f); }
 float kto_nt_factor(float r, float a_norm, float r_isco, float inv_m) { return nt_factor(r, a_norm, r_isco, inv_m); }
 double kto_define_value(float v) { return define_value(v); }
 uint32_t kto_pcg32(uint64_t state) { return pcg32(state); }

@@ -7,7 +7,7 @@
 // (src/renderer/init.rs:112-118).  The C functions below redo what the Rust host does around
 // the kernels: upload c_params (init.rs:129-139), create the two LUT textures
 // (texture.rs:86-202) and launch trace_kernel / bloom_horizontal / post_process with the
-// arguments of submit_render (mod.rs:547-600).  The outputs are the GPU golden the tests and
+// arguments of submit_render (mod.rs:153-206).  The outputs are the GPU golden the tests and
 // the reference arm of bench.py compare against; nothing here is shipped.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -73,7 +73,7 @@ int ktref_free_textures(ktref_textures* t) {
     return 0;
 }
 
-// mod.rs:547-567
+// mod.rs:153-173
 int ktref_trace(float* hdr, int width, int height, const float* cam12, unsigned long long lut_tex, int lut_size,
                 float max_temp, unsigned int* err, unsigned long long disk_tex, float disk_inner, float disk_outer,
                 float fov_scale, int bx, int by, void* stream) {
@@ -85,7 +85,7 @@ int ktref_trace(float* hdr, int width, int height, const float* cam12, unsigned 
     return (int)cudaGetLastError();
 }
 
-// mod.rs:571-585
+// mod.rs:177-191
 int ktref_bloom(const float* hdr, float* bloom, int width, int height, int radius, float sigma, int enabled, int bx,
                 int by, void* stream) {
     dim3 block(bx, by), grid((width + bx - 1) / bx, (height + by - 1) / by);
@@ -94,7 +94,7 @@ int ktref_bloom(const float* hdr, float* bloom, int width, int height, int radiu
     return (int)cudaGetLastError();
 }
 
-// mod.rs:586-600 with the shared-memory size of mod.rs:669-686
+// mod.rs:192-206 with the shared-memory size of mod.rs:275-292
 int ktref_post(const float* hdr, const float* bloom, unsigned int* image, int width, int height, int radius,
                float sigma, float intensity, int enabled, int bx, int by, void* stream) {
     dim3 block(bx, by), grid((width + bx - 1) / bx, (height + by - 1) / by);

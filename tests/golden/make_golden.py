@@ -27,20 +27,18 @@ FIXTURES = {"t1": None, "t2": None, "c1": (64, 64), "c2": (192, 108)}
 def main(out: Path) -> None:
     import torch
 
-    import kerrtrace_b200 as kt
     import oracle
     from kerrtrace_b200 import workloads
 
+    host = oracle.Host()
     out.mkdir(parents=True, exist_ok=True)
     meta = {}
     for name, size in FIXTURES.items():
-        cfg, cam = workloads.scene(name)
+        cfg, cam = workloads.scene(name, host=host)
         if size:
             cfg = workloads.scaled(cfg, *size)
-        p = kt.build_kerr_params(cfg)
-        bb = kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start, cfg.wavelength_end,
-                                       cfg.wavelength_step)
-        disk = kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)
+        # the reference host's inputs from the oracle's restatement (no product code on this path)
+        p, bb, disk = oracle.reference_inputs(cfg)
         ref = oracle.RefKernel(name)
         ref.setup(p, bb, disk)
         n = cfg.width * cfg.height

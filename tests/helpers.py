@@ -22,12 +22,11 @@ def run_ours(torch, cfg, cam, schedule=kt.SCHED_WAVEFRONT, counted=False, ctx=No
 
 
 def run_ref(torch, scene: str, cfg, cam):
-    """The reference's trace_kernel on the same inputs (defines of `scene`, runtime cfg/cam)."""
+    """The reference's trace_kernel on the same inputs (defines of `scene`, runtime cfg/cam).
+    Its KerrParams and LUTs come from the oracle's restatement of the reference host, not from
+    the product, so a bit-identical image also pins the product's host tables."""
     import oracle
-    p = kt.build_kerr_params(cfg)
-    bb = kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start, cfg.wavelength_end,
-                                   cfg.wavelength_step)
-    disk = kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)
+    p, bb, disk = oracle.reference_inputs(cfg)
     ref = oracle.RefKernel(scene)
     ref.setup(p, bb, disk)
     n = cfg.width * cfg.height

@@ -33,7 +33,7 @@ def test_every_declared_symbol_is_exported(kt):
 
 def test_library_loads_and_versions(kt):
     L = kt.lib()
-    assert L.kt_abi_version() == 2
+    assert L.kt_abi_version() == 3
     assert L.kt_status_str(kt.KT_ERR_LUT_OVERFLOW).decode().startswith("colour temperature")
 
 
@@ -217,3 +217,71 @@ def test_diff_rejects_unsupported_configurations(kt):
         setattr(c, field, value)
         with pytest.raises(kt.KtError):
             kt.Diff(c, view)
+
+
+def _struct_bytes(s) -> bytes:
+    return bytes(C.string_at(C.addressof(s), C.sizeof(s)))
+
+
+def test_oracle_host_restatement_equals_the_library_host(kt, orc):
+    """The runs of the reference kernel take their scene values, KerrParams, LUTs and cameras
+    from the oracle's restatement of the reference host (oracle.Host, oracle.reference_inputs);
+    the tests and the bench arm of the product take them from the library.  Both restatements
+    must give the same bits for every named scene, else the two arms would not see one scene."""
+    from kerrtrace_b200 import workloads
+    host = orc.Host()
+    assert _struct_bytes(host.config_default()) == _struct_bytes(kt.config_default())
+    for name in workloads.SCENES:
+        c_lib, cam_lib = workloads.scene(name)
+        c_orc, cam_orc = workloads.scene(name, host=host)
+        assert _struct_bytes(c_lib) == _struct_bytes(c_orc), name
+        assert _struct_bytes(cam_lib) == _struct_bytes(cam_orc), name
+        p_orc, bb, dk = orc.reference_inputs(c_orc)
+        assert _struct_bytes(p_orc) == _struct_bytes(kt.build_kerr_params(c_lib)), name
+        bb_lib = kt.generate_blackbody_lut(c_lib.lut_size, c_lib.lut_max_temp, c_lib.wavelength_start,
+                                           c_lib.wavelength_end, c_lib.wavelength_step)
+        dk_lib = kt.generate_disk_lut(kt.build_kerr_params(c_lib), c_lib.disk_outer_radius, c_lib.lut_size)
+        assert np.array_equal(bb.view(np.uint32), bb_lib.view(np.uint32)), name
+        assert np.array_equal(dk.view(np.uint32), dk_lib.view(np.uint32)), name
+    for (c1, k1), (c2, k2) in zip(workloads.c4_jobs(), workloads.c4_jobs(host=host)):
+        assert _struct_bytes(c1) == _struct_bytes(c2) and _struct_bytes(k1) == _struct_bytes(k2)
+    rng = np.random.default_rng(11)
+    for yaw, pitch in zip(rng.uniform(-180, 180, 200), rng.uniform(-89, 89, 200)):
+        assert kt.camera_basis(float(yaw), float(pitch)) == orc.camera_basis(float(yaw), float(pitch))
+    for fov in rng.uniform(1.0, 120.0, 200):
+        assert np.float32(kt.lib().kt_fov_scale(float(fov))) == np.float32(orc.fov_scale(float(fov)))
+
+
+@pytest.mark.gpu
+def test_autotune_through_the_c_abi(kt):
+    """kt_context_autotune (C++, CUDA events) on the 1080p scene at 320 x 180: every candidate of
+    the built-in list is timed, all give the default shape's image bit for bit, and the
+    installed tuning (KT_SCHED_AUTO) reproduces that image."""
+    import torch
+    from kerrtrace_b200 import workloads
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    cfg, cam = workloads.scene("c2")
+    cfg = workloads.scaled(cfg, 320, 180)
+    ctx = kt.Context(cfg)
+    n = cfg.width * cfg.height
+    base = torch.zeros((n, 4), device="cuda")
+    out = torch.zeros((n, 4), device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    ctx.trace(base_cam := cam, base.data_ptr(), err.data_ptr(), 0, kt.SCHED_WAVEFRONT)
+    table = (kt.KtTuneEntry * kt.TUNE_MAX_CANDIDATES)()
+    n_rows = C.c_uint32(0)
+    kt.check(kt.lib().kt_context_autotune(ctx.handle, None, C.byref(base_cam), 2, None, 0, table, C.byref(n_rows)))
+    rows = [table[i] for i in range(n_rows.value)]
+    assert len(rows) == 56  # FP32 reference semantics: 2 orders x (6 + 6 plain + 16 wavefront)
+    assert all(r.identical == 1 and r.ms > 0 for r in rows)
+    best = ctx.tuning()
+    assert min(r.ms for r in rows) == next(r.ms for r in rows if r.tuning.as_dict() == best.as_dict())
+    ctx.trace(cam, out.data_ptr(), err.data_ptr(), 0, kt.SCHED_AUTO)
+    torch.cuda.synchronize()
+    assert torch.equal(out.view(torch.int32), base.view(torch.int32))
+    bad = kt.KtTuning(kt.SCHED_PLAIN, 0, 0, 4, 1, 0, 0)
+    assert kt.lib().kt_context_autotune(ctx.handle, None, C.byref(cam), 0, None, 0, None, None) == kt.KT_ERR_INVALID_ARG
+    assert kt.lib().kt_context_autotune(ctx.handle, None, C.byref(cam), 1, C.byref(bad), 0, None, None) == \
+        kt.KT_ERR_INVALID_ARG
+    ctx.close()

@@ -23,11 +23,10 @@ def _rank(rank: int, world: int, port: int, out):
     import torch.distributed as dist
 
     import bench
-    import kerrtrace_b200 as kt
     from kerrtrace_b200 import workloads
     try:
         r, w, local = bench.dist_setup("gloo")
-        cfg, cam = bench.rank_camera(kt, workloads, "c2", r, w)
+        cfg, cam = bench.rank_camera(workloads, "c2", r, w)
         bench.barrier(w)
         t_max = bench.max_over_ranks(10.0 * (r + 1), w)      # rank 1 is the slower one
         out.put((r, list(cam.cam_pos), list(cam.fwd), cam.fov_scale, cfg.width * cfg.height, t_max,

@@ -29,9 +29,9 @@ def test_ring_and_order(cuda):
     args = (list(cam.cam_pos), list(cam.fwd), list(cam.rgt), list(cam.up), cam.fov_scale)
     assert r.submit_render(*args)
     assert r.submit_render(*args)
-    assert not r.submit_render(*args)          # both frames in flight (mod.rs:521-523)
+    assert not r.submit_render(*args)          # both frames in flight (mod.rs:127-129)
     with pytest.raises(kt.KtError) as e:
-        r.finish_frame(1)                      # out of order (mod.rs:646-650)
+        r.finish_frame(1)                      # out of order (mod.rs:253-256)
     assert e.value.status == kt.KT_ERR_QUEUE_ORDER
     i0, img0 = _wait_ready(r)
     img0 = img0.copy()

@@ -6,7 +6,6 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-import kerrtrace_b200 as kt
 from kerrtrace_b200 import workloads
 
 pytestmark = pytest.mark.gpu
@@ -30,10 +29,7 @@ def emulate(lut, u, mode):
 
 def test_texture_model(cuda, orc):
     cfg, _ = workloads.scene("t1")
-    p = kt.build_kerr_params(cfg)
-    bb = kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start, cfg.wavelength_end,
-                                   cfg.wavelength_step)
-    disk = kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)
+    p, bb, disk = orc.reference_inputs(cfg)
     ref = orc.RefKernel("t1")
     ref.setup(p, bb, disk)
     rng = np.random.default_rng(3)

@@ -198,3 +198,41 @@ def test_large_frame_matches_reference_kernel(cuda):
         a, b = ours[diff, :3].astype(np.float64), ref[diff, :3].astype(np.float64)
         assert np.all(np.abs(a - b) <= 1e-5 * np.abs(b).max(1, keepdims=True))
     assert np.array_equal(err_o, err_r)
+
+
+def test_c1_full_frame_matches_reference_kernel(cuda):
+    """The plain-method benchmark scene at its full 256 x 256 (tolerance 1e-8, a = 0.9) against
+    the reference's trace_kernel on the same inputs."""
+    cfg, cam = workloads.scene("c1")
+    ours, err_o, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_WAVEFRONT)
+    ref, err_r = run_ref(cuda, "c1", cfg, cam)
+    r = compare_hdr(ours, ref, cfg.width, cfg.height)
+    print(r)
+    assert r["class_mismatch_inner"] == 0, r
+    assert r["over_tol_all"] == 0, r
+    assert r["bit_equal"] >= 1.0 - 1e-4, r
+    assert np.array_equal(err_o, err_r)
+
+
+@pytest.mark.parametrize("schedule", [kt.SCHED_PLAIN, kt.SCHED_WAVEFRONT])
+def test_keep_frozen_rays_is_bit_identical(cuda, schedule):
+    """Tuning keep_frozen = 1 lets rays whose state became NaN iterate to max_steps, as the
+    reference's do (cuda/kerr_trace.cuh:62,83-125).  The image is the one of the default
+    (retiring) kernel and of the reference kernel, bit for bit; only the work grows."""
+    cfg, cam = workloads.scaled(workloads.scene("c2")[0], 256, 144), workloads.scene("c2")[1]
+    ctx = kt.Context(cfg)
+    ctx.set_tuning(schedule=schedule, block_x=16, block_y=8)
+    a, ea, sa, _ = run_ours(cuda, cfg, cam, schedule, counted=True, ctx=ctx)
+    ctx.set_tuning(schedule=schedule, block_x=16, block_y=8, keep_frozen=1)
+    assert ctx.tuning().keep_frozen == 1
+    b, eb, sb, _ = run_ours(cuda, cfg, cam, schedule, counted=True, ctx=ctx)
+    c, _, _, _ = run_ours(cuda, cfg, cam, schedule, ctx=ctx)
+    ref, err_r = run_ref(cuda, "c2", cfg, cam)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(b.view(np.uint32), c.view(np.uint32))
+    assert np.array_equal(a.view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(ea, eb) and np.array_equal(ea, err_r)
+    assert sa.frozen_rays == sb.frozen_rays > 0
+    # every frozen ray now runs out its step budget
+    assert sb.steps - sa.steps >= sb.frozen_rays * cfg.max_steps // 2, (sa.steps, sb.steps, sb.frozen_rays)
+    ctx.close()

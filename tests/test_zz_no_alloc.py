@@ -81,6 +81,57 @@ def test_noalloc_matches_context_entry_point(cuda, name, size):
     ctx.close()
 
 
+def _luts(torch, cfg):
+    p = kt.build_kerr_params(cfg)
+    bb = torch.from_numpy(kt.generate_blackbody_lut(cfg.lut_size, cfg.lut_max_temp, cfg.wavelength_start,
+                                                    cfg.wavelength_end, cfg.wavelength_step)).cuda()
+    disk = torch.from_numpy(kt.generate_disk_lut(p, cfg.disk_outer_radius, cfg.lut_size)).cuda()
+    return bb, disk
+
+
+def _check_views(torch, cfg, cams, hdr, err):
+    """Every pixel of every view written (alpha 1 over the -1 fill) and equal to kt_trace's image
+    of that view to the parity tolerance."""
+    ctx = kt.Context(cfg)
+    try:
+        for v, c in enumerate(cams):
+            assert np.all(hdr[v][:, 3] == 1.0), v
+            exp_hdr, exp_err = _with_context(torch, ctx, cfg, c)
+            r = compare_hdr(hdr[v], exp_hdr, cfg.width, cfg.height)
+            assert r["class_mismatch_inner"] == 0, (v, r)
+            assert r["over_tol_inner"] == 0, (v, r)
+            assert r["over_tol_all"] <= max(2, 0.005 * r["n"]), (v, r)
+            assert np.array_equal(err[v], exp_err)
+    finally:
+        ctx.close()
+
+
+def test_noalloc_rays_without_work_fill_every_view(cuda):
+    """max_steps = 0: no pixel has ray work, so every claim of every warp comes back without an
+    active lane; warps must keep claiming until all views are written."""
+    cfg, cam = workloads.scene("c2")
+    cfg = workloads.scaled(cfg, 256, 144)
+    cfg.max_steps = 0
+    bb, disk = _luts(cuda, cfg)
+    cams = _views(cam, 3)
+    hdr, err, _ = _noalloc(cuda, cfg, cams, bb, disk)
+    assert np.all(hdr[:, :, :3] == 0.0)
+    _check_views(cuda, cfg, cams, hdr, err)
+
+
+@pytest.mark.parametrize("n_views,size", [(8, (320, 256)), (64, (32, 32))])
+def test_noalloc_many_views(cuda, n_views, size):
+    """8 views of a frame larger than one resident wave of the persistent grid (148 SMs x 4
+    blocks x 128 lanes = 75 776 < 81 920 pixels), and 64 views smaller than one wave, where most
+    warps find their first view used up on their first claim."""
+    cfg, cam = workloads.scene("t1")
+    cfg = workloads.scaled(cfg, *size)
+    bb, disk = _luts(cuda, cfg)
+    cams = _views(cam, n_views)
+    hdr, err, _ = _noalloc(cuda, cfg, cams, bb, disk)
+    _check_views(cuda, cfg, cams, hdr, err)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
     cfg, cam = workloads.scene("t2")
     dummy = cuda.zeros(16, device="cuda")
