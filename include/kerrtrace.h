@@ -342,7 +342,8 @@ void kt_batch_destroy(kt_batch* b);
  * model of the texture unit's filter, so its images match kt_trace to the parity tolerance.
  * The first call on a device looks up the scratch array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture.  Every call shares the scratch: calls that overlap on the GPU race and must be
+ * capture.  The address is kept for the life of the process: after a cudaDeviceReset of that
+ * device (which unloads the library's device image) do not call this entry point on it again.  Every call shares the scratch: calls that overlap on the GPU race and must be
  * serialised by the caller.
  */
 kt_status kt_trace_noalloc(const kt_config* cfg, const kt_camera* cams, uint32_t n_views,
