@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-c3", action="store_true", help="skip the 4096^2 x 8-draw precision ablation")
     ap.add_argument("--no-sequence", action="store_true", help="skip the headless frame-sequence leg")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-pareto", action="store_true",
+                    help="skip the accuracy-against-speed sweep of FP32 / mixed / FP64 over tolerances")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -330,6 +332,88 @@ def precision_leg(cfg, cam, local, reps: int) -> dict:
     return runs
 
 
+PARETO_TOLERANCES = (1e-5, 1e-6, 1e-7, 1e-8, 1e-9)
+
+
+def pareto_leg(local, reference_tol: float = 1e-10, c3_size: int = 2048) -> dict:
+    """Accuracy against speed of FP32, mixed precision and FP64 (stated physics) on three scenes:
+    the 1080p frame (c2) and draws 0 and 1 of the mixed-precision ablation at c3_size^2.  Each
+    scene is first traced in FP64 at `reference_tol` (the converged image); then every precision
+    at each tolerance of PARETO_TOLERANCES gives an event-timed trace (launch shape tuned once per
+    scene and precision at tolerance 1e-6) and its per-pixel HDR error against the converged
+    image (p99, p99.9, fraction above 1e-3; relative per pixel, floor 1e-6 x the image maximum).
+    `at_equal_accuracy` lists, per scene and error target, the fastest tolerance of each
+    precision whose p99 meets the target."""
+    import torch
+
+    import kerrtrace_b200 as kt
+    from kerrtrace_b200 import autotune, workloads
+
+    stream = torch.cuda.current_stream().cuda_stream
+    scenes = [("c2", *workloads.scene("c2"))]
+    for dr in (0, 1):
+        c, cam = workloads.c3(dr, c3_size)
+        scenes.append((f"c3_draw{dr}_{c3_size}", c, cam))
+    precs = (("fp32", kt.PREC_FP32), ("mixed", kt.PREC_MIXED), ("fp64", kt.PREC_FP64))
+    out = {"reference_tolerance": reference_tol, "tolerances": list(PARETO_TOLERANCES), "scenes": {}}
+    for name, cfg0, cam in scenes:
+        cfg0 = cfg0.copy()
+        cfg0.mode = kt.MODE_SPEC
+        n = cfg0.width * cfg0.height
+        hdr = torch.zeros((n, 4), device="cuda")
+        ref = torch.zeros((n, 4), device="cuda")
+        err = torch.zeros(2, dtype=torch.int32, device="cuda")
+        c = cfg0.copy()
+        c.precision, c.tolerance = kt.PREC_FP64, reference_tol
+        ctx = kt.Context(c, local)
+        ctx.set_tuning(schedule=kt.SCHED_WAVEFRONT, blocks_per_sm=4)
+        ctx.trace(cam, ref.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+        torch.cuda.synchronize()
+        ctx.close()
+        r = ref[:, :3].double()
+        floor = 1e-6 * float(r.abs().max())
+        rows = []
+        for pname, prec in precs:
+            tuning = None
+            for tol in PARETO_TOLERANCES:
+                c = cfg0.copy()
+                c.precision, c.tolerance = prec, tol
+                ctx = kt.Context(c, local)
+                if tuning is None:
+                    t6 = cfg0.copy()
+                    t6.precision, t6.tolerance = prec, 1e-6
+                    tctx = kt.Context(t6, local)
+                    tuning = autotune.autotune(tctx, cam, reps=1, stream=stream).best
+                    tctx.close()
+                ctx.set_tuning(**tuning)
+                st = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(2):
+                    ctx.trace(cam, hdr.data_ptr(), err.data_ptr(), stream, kt.SCHED_AUTO)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / 2
+                rel = ((hdr[:, :3].double() - r).abs() / r.abs().clamp_min(floor)).max(1).values
+                q = torch.quantile(rel.float()[torch.randperm(n, device="cuda")[:min(n, 1 << 24)]],
+                                   torch.tensor([0.99, 0.999], device="cuda"))
+                rows.append({"precision": pname, "tolerance": tol, "trace_ms": round(ms, 4),
+                             "mrays_s": round(n * c.spp / ms / 1e3, 1), "steps": int(st.steps),
+                             "hdr_p99": float(q[0]), "hdr_p999": float(q[1]),
+                             "hdr_frac_over_1e-3": float((rel > 1e-3).double().mean())})
+                ctx.close()
+        best = {}
+        for target in (1e-4, 1e-5, 1e-6):
+            best[f"p99<={target:g}"] = {}
+            for pname, _ in precs:
+                ok = [x for x in rows if x["precision"] == pname and x["hdr_p99"] <= target]
+                f = min(ok, key=lambda x: x["trace_ms"]) if ok else None
+                best[f"p99<={target:g}"][pname] = (
+                    {"tolerance": f["tolerance"], "trace_ms": f["trace_ms"], "mrays_s": f["mrays_s"]} if f else None)
+        out["scenes"][name] = {"size": f"{cfg0.width}x{cfg0.height}", "points": rows, "at_equal_accuracy": best}
+    return out
+
+
 def _log_hist(x, hist, lo: float = -12.0, bins: int = 1300):
     """Accumulate log10 of positive relative errors into 0.01-decade bins (zeros into bin 0)."""
     import torch
@@ -500,9 +584,10 @@ def sequence_leg(cfg, tuning, local, moving: int = 60, resting: int = 30) -> dic
 
 def batch_leg(local, reps: int) -> dict:
     """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
-    random spins, inclinations, observer and disk radii): one batched launch at the fastest of
-    six block shapes, the same launch replayed from a CUDA graph, and the baseline of 64
-    sequential plain launches; then the same renders in stated physics and mixed precision."""
+    random spins, inclinations, observer and disk radii): one batched launch in the shape the
+    batch tuner picks (plain block shapes or the persistent launch), the same launch replayed from
+    a CUDA graph, and the baseline of 64 sequential plain launches; then the same renders in
+    stated physics and mixed precision."""
     import torch
 
     import kerrtrace_b200 as kt
@@ -515,21 +600,12 @@ def batch_leg(local, reps: int) -> dict:
     rays = b.rays()
     stream = torch.cuda.current_stream().cuda_stream
     out = {"jobs": len(jobs), "rays": rays}
-    # block shape of the batched launch: the fastest of the plain shapes (one launch each)
-    shapes = {}
-    for bx, by in ((16, 16), (32, 8), (8, 8), (16, 8), (8, 16), (32, 4)):
-        b.set_block(bx, by)
-        b.trace(stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        b.trace(stream)
-        e1.record()
-        torch.cuda.synchronize()
-        shapes[f"{bx}x{by}"] = round(e0.elapsed_time(e1), 3)
-    best = min(shapes, key=shapes.get)
-    b.set_block(*(int(v) for v in best.split("x")))
-    out["block_ms"] = shapes
-    out["block"] = best
+    # launch shape of the batched launch: kt_batch_autotune (plain block shapes and the persistent
+    # launch of job-uniform 32-pixel units), every candidate checked bit for bit
+    rows = b.autotune(reps=2, stream=stream)
+    out["tuner"] = [{"ms": round(ms, 3), **{k: t[k] for k in ("schedule", "block_x", "block_y", "blocks_per_sm")},
+                     "identical": ok} for ms, t, ok in rows]
+    out["tuning"] = b.tuning().as_dict()
     for name, fn in (("sequential_plain", lambda: b.trace_sequential(stream, kt.SCHED_PLAIN)),
                      ("batched_launch", lambda: b.trace(stream)),
                      ("batched_graph", lambda: b.trace_graph(stream))):
@@ -552,7 +628,8 @@ def batch_leg(local, reps: int) -> dict:
         c.mode, c.precision = kt.MODE_SPEC, kt.PREC_MIXED
         mjobs.append((c, cam))
     mb = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(mjobs, bufs)], local)
-    mb.set_block(*(int(v) for v in best.split("x")))
+    out["mixed_tuner"] = [{"ms": round(ms, 3), **{k: t[k] for k in ("schedule", "block_x", "block_y", "blocks_per_sm")},
+                           "identical": ok} for ms, t, ok in mb.autotune(reps=1, stream=stream)]
     mb.trace_graph(stream)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -781,6 +858,7 @@ def run_ours(args, rank, world, local):
             ("precision", args.no_precision, lambda: precision_leg(cfg, cam, local, max(3, args.steps))),
             ("adjoint", args.no_adjoint, lambda: adjoint_leg(local, max(3, args.steps))),
             ("batch", args.no_batch, lambda: batch_leg(local, 3)),
+            ("pareto", args.no_pareto, lambda: pareto_leg(local)),
             ("sequence", args.no_sequence, lambda: sequence_leg(cfg, ctx.tuning(), local)),
             ("c3", args.no_c3, lambda: c3_leg(local))]
     for name, skip, run in legs:

@@ -310,6 +310,20 @@ typedef struct kt_batch kt_batch;
 kt_status kt_batch_create(const kt_job* jobs, uint32_t n_jobs, int device, kt_batch** out);
 /* Plain-schedule block shape of the batched launch (default 16x16; at most 1024 threads). */
 kt_status kt_batch_set_block(kt_batch* b, int32_t block_x, int32_t block_y);
+/* Launch shape of the batch.  schedule KT_SCHED_PLAIN: one thread per pixel on tiles of
+ * block_x x block_y (as kt_batch_set_block).  KT_SCHED_WAVEFRONT: one persistent launch of
+ * 128-thread blocks (blocks_per_sm resident per SM, 4..6; only the FP32 reference-semantics
+ * kernel has 5 and 6) whose warps take 32-pixel units, each inside one job, from one device
+ * counter over all jobs.  Both give every job the image of its own kt_trace, bit for bit. */
+kt_status kt_batch_set_tuning(kt_batch* b, const kt_tuning* tuning);
+kt_status kt_batch_get_tuning(const kt_batch* b, kt_tuning* tuning);
+/* Times the batched launch under each candidate shape (six plain block shapes, the persistent
+ * launch at each blocks_per_sm it has) with CUDA events on `stream` (one launch to compare the
+ * images with the first candidate's, then `reps` timed launches, median), and installs the
+ * fastest whose images of every job equal the first candidate's bit for bit.  table (may be
+ * NULL; room for KT_TUNE_MAX_CANDIDATES rows) and *n_entries as kt_context_autotune.  Allocates
+ * a copy of all job images and synchronises `stream`: call it at set-up, outside capture. */
+kt_status kt_batch_autotune(kt_batch* b, void* stream, uint32_t reps, kt_tune_entry* table, uint32_t* n_entries);
 /* New camera for job j (the next kt_batch_trace_graph re-captures its graph). */
 kt_status kt_batch_set_camera(kt_batch* b, uint32_t j, const kt_camera* cam);
 /* Traces every job in one kernel launch on `stream`. */

@@ -207,6 +207,9 @@ SIGNATURES = [
     ("kt_batch_create", C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
     ("kt_batch_set_block", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     ("kt_batch_set_camera", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(KtCamera)]),
+    ("kt_batch_set_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
+    ("kt_batch_get_tuning", C.c_int, [C.c_void_p, C.POINTER(KtTuning)]),
+    ("kt_batch_autotune", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),
     ("kt_batch_trace", C.c_int, [C.c_void_p, C.c_void_p]),
     ("kt_batch_trace_graph", C.c_int, [C.c_void_p, C.c_void_p]),
     ("kt_batch_trace_sequential", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
@@ -501,6 +504,26 @@ class Batch:
 
     def set_camera(self, j: int, cam: KtCamera):
         check(lib().kt_batch_set_camera(self.handle, j, C.byref(cam)))
+
+    def set_tuning(self, schedule: int = SCHED_PLAIN, block_x: int = 16, block_y: int = 16, blocks_per_sm: int = 4,
+                   **_ignored):
+        """SCHED_PLAIN: tiles of block_x x block_y; SCHED_WAVEFRONT: the persistent launch of
+        32-pixel units with blocks_per_sm resident 128-thread blocks per SM."""
+        t = KtTuning(schedule, block_x, block_y, blocks_per_sm, 1, 0, 0)
+        check(lib().kt_batch_set_tuning(self.handle, C.byref(t)))
+
+    def tuning(self) -> KtTuning:
+        t = KtTuning()
+        check(lib().kt_batch_get_tuning(self.handle, C.byref(t)))
+        return t
+
+    def autotune(self, reps: int = 3, stream: int = 0) -> list:
+        """kt_batch_autotune: installs the fastest bit-identical launch shape; returns the rows
+        (ms, tuning dict, identical)."""
+        table = (KtTuneEntry * TUNE_MAX_CANDIDATES)()
+        n = C.c_uint32(0)
+        check(lib().kt_batch_autotune(self.handle, C.c_void_p(stream), reps, table, C.byref(n)))
+        return [(float(table[i].ms), table[i].tuning.as_dict(), bool(table[i].identical)) for i in range(n.value)]
 
     def trace(self, stream: int = 0):
         check(lib().kt_batch_trace(self.handle, C.c_void_p(stream)))

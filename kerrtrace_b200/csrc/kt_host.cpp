@@ -15,6 +15,7 @@
 // Device context and renderer follow src/renderer/{texture,init,mod}.rs.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <charconv>
 #include <cmath>
 #include <cstdarg>
@@ -1132,6 +1133,9 @@ struct kt_batch {
     std::vector<kt_job> jobs;
     ktd::BatchTable* table = nullptr;
     int bx = 16, by = 16;
+    int schedule = KT_SCHED_PLAIN;  // KT_SCHED_PLAIN: tiles of bx x by; KT_SCHED_WAVEFRONT: persistent units
+    int blocks_per_sm = 4;          // persistent launch: resident 128-thread blocks per SM
+    unsigned* counter = nullptr;    // persistent launch: the unit counter (1 word)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t capture = nullptr;
@@ -1146,14 +1150,22 @@ void batch_drop_graph(kt_batch* b) {
 }
 void batch_layout(kt_batch* b) {
     int tiles = 0;
+    unsigned units = 0;
     for (int j = 0; j < b->table->n; ++j) {
         ktd::BatchJob& e = b->table->job[j];
         e.tiles_x = (e.sc.width + b->bx - 1) / b->bx;
         const int tiles_y = (e.sc.height + b->by - 1) / b->by;
         e.tile_begin = tiles;
         tiles += e.tiles_x * tiles_y;
+        e.unit_begin = units;
+        units += (unsigned)(((uint64_t)e.sc.width * e.sc.height + 31) / 32);
     }
     b->table->total_tiles = tiles;
+    b->table->total_units = units;
+}
+cudaError_t batch_launch(kt_batch* b, cudaStream_t st) {
+    if (b->schedule == KT_SCHED_WAVEFRONT) return ktd::launch_batch_persistent(*b->table, b->blocks_per_sm, b->counter, st);
+    return ktd::launch_batch(*b->table, b->bx, b->by, st);
 }
 void batch_free(kt_batch* b) {
     if (!b) return;
@@ -1161,6 +1173,7 @@ void batch_free(kt_batch* b) {
         DeviceGuard g(b->device);
         batch_drop_graph(b);
         if (b->capture) cudaStreamDestroy(b->capture);
+        cudaFree(b->counter);
     }
     for (kt_context* c : b->ctx) destroy_ctx(c);
     delete b->table;
@@ -1205,6 +1218,14 @@ kt_status kt_batch_create(const kt_job* jobs, uint32_t n, int device, kt_batch**
         e.err = jobs[j].err_word;
     }
     batch_layout(b);
+    {
+        DeviceGuard g(device);
+        const cudaError_t e = cudaMalloc(&b->counter, sizeof(unsigned));
+        if (e != cudaSuccess) {
+            batch_free(b);
+            return cuda_fail(e, "allocate the unit counter");
+        }
+    }
     *out = b;
     return KT_OK;
 }
@@ -1214,8 +1235,33 @@ kt_status kt_batch_set_block(kt_batch* b, int32_t bx, int32_t by) {
     if (bx <= 0 || by <= 0 || (int64_t)bx * by > 1024) return fail(KT_ERR_INVALID_ARG, "block %dx%d invalid", bx, by);
     b->bx = bx;
     b->by = by;
+    b->schedule = KT_SCHED_PLAIN;
     batch_layout(b);
     batch_drop_graph(b);
+    return KT_OK;
+}
+
+kt_status kt_batch_set_tuning(kt_batch* b, const kt_tuning* t) {
+    if (!b || !t) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (t->schedule == KT_SCHED_PLAIN) return kt_batch_set_block(b, t->block_x, t->block_y);
+    if (t->schedule != KT_SCHED_WAVEFRONT)
+        return fail(KT_ERR_INVALID_ARG, "batch tuning schedule %d must be plain or wavefront", t->schedule);
+    if (t->blocks_per_sm < 4 || t->blocks_per_sm > 6)
+        return fail(KT_ERR_INVALID_ARG, "batch blocks_per_sm %d not in 4..6", t->blocks_per_sm);
+    b->schedule = KT_SCHED_WAVEFRONT;
+    b->blocks_per_sm = t->blocks_per_sm;
+    batch_drop_graph(b);
+    return KT_OK;
+}
+
+kt_status kt_batch_get_tuning(const kt_batch* b, kt_tuning* t) {
+    if (!b || !t) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    std::memset(t, 0, sizeof *t);
+    t->schedule = b->schedule;
+    t->block_x = b->schedule == KT_SCHED_PLAIN ? b->bx : 0;
+    t->block_y = b->schedule == KT_SCHED_PLAIN ? b->by : 0;
+    t->blocks_per_sm = b->schedule == KT_SCHED_WAVEFRONT ? b->blocks_per_sm : 4;
+    t->refill_min = 1;
     return KT_OK;
 }
 
@@ -1231,7 +1277,7 @@ kt_status kt_batch_set_camera(kt_batch* b, uint32_t j, const kt_camera* cam) {
 kt_status kt_batch_trace(kt_batch* b, void* stream) {
     if (!b) return fail(KT_ERR_INVALID_ARG, "batch is NULL");
     DeviceGuard g(b->device);
-    const cudaError_t e = ktd::launch_batch(*b->table, b->bx, b->by, (cudaStream_t)stream);
+    const cudaError_t e = batch_launch(b, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "batch launch");
     return KT_OK;
 }
@@ -1242,7 +1288,7 @@ kt_status kt_batch_trace_graph(kt_batch* b, void* stream) {
     if (!b->exec) {
         if (!b->capture) KT_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking), "create capture stream");
         KT_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal), "begin capture");
-        const cudaError_t le = ktd::launch_batch(*b->table, b->bx, b->by, b->capture);
+        const cudaError_t le = batch_launch(b, b->capture);
         cudaGraph_t graph = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(b->capture, &graph);
         if (le != cudaSuccess) {
@@ -1258,6 +1304,106 @@ kt_status kt_batch_trace_graph(kt_batch* b, void* stream) {
         }
     }
     KT_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream), "launch graph");
+    return KT_OK;
+}
+
+kt_status kt_batch_autotune(kt_batch* b, void* stream, uint32_t reps, kt_tune_entry* table, uint32_t* n_entries) {
+    if (!b) return fail(KT_ERR_INVALID_ARG, "batch is NULL");
+    if (reps == 0 || reps > 64) return fail(KT_ERR_INVALID_ARG, "kt_batch_autotune: reps must be in 1..64");
+    DeviceGuard g(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    kt_tuning saved;
+    kt_batch_get_tuning(b, &saved);
+    std::vector<kt_tuning> cands;
+    static const int kPlain[][2] = {{16, 16}, {32, 8}, {8, 8}, {16, 8}, {8, 16}, {32, 4}};
+    for (const auto& s2 : kPlain) {
+        kt_tuning t{};
+        t.schedule = KT_SCHED_PLAIN;
+        t.block_x = s2[0];
+        t.block_y = s2[1];
+        t.blocks_per_sm = 4;
+        t.refill_min = 1;
+        cands.push_back(t);
+    }
+    const bool variants = b->jobs[0].cfg.precision == KT_PREC_FP32 && b->jobs[0].cfg.mode == KT_MODE_REF;
+    for (int bps = 4; bps <= (variants ? 6 : 4); ++bps) {
+        kt_tuning t{};
+        t.schedule = KT_SCHED_WAVEFRONT;
+        t.blocks_per_sm = bps;
+        t.refill_min = 1;
+        cands.push_back(t);
+    }
+    // first candidate's images of every job, kept for the bit-identity test of the others
+    size_t total = 0;
+    for (const kt_job& j : b->jobs) total += (size_t)j.cfg.width * j.cfg.height;
+    float4* keep = nullptr;
+    unsigned long long* diff = nullptr;
+    std::vector<cudaEvent_t> ev(2 * reps, nullptr);
+    auto release = [&]() {
+        cudaFree(keep);
+        cudaFree(diff);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&keep, total * sizeof(float4))) != cudaSuccess ||
+        (e = cudaMalloc(&diff, sizeof(unsigned long long))) != cudaSuccess) {
+        release();
+        return cuda_fail(e, "kt_batch_autotune: allocate scratch");
+    }
+    for (cudaEvent_t& x : ev)
+        if ((e = cudaEventCreate(&x)) != cudaSuccess) {
+            release();
+            return cuda_fail(e, "kt_batch_autotune: create events");
+        }
+    std::vector<kt_tune_entry> rows;
+    kt_status out = KT_OK;
+    for (size_t i = 0; i < cands.size() && out == KT_OK; ++i) {
+        if ((out = kt_batch_set_tuning(b, &cands[i])) != KT_OK) break;
+        if ((e = batch_launch(b, st)) != cudaSuccess) { out = cuda_fail(e, "kt_batch_autotune: launch"); break; }
+        unsigned long long mism = 0;
+        size_t off = 0;
+        for (const kt_job& j : b->jobs) {
+            const size_t n = (size_t)j.cfg.width * j.cfg.height;
+            if (i == 0) {
+                e = cudaMemcpyAsync(keep + off, j.hdr_out, n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+            } else {
+                unsigned long long d = 0;
+                if ((e = ktd::launch_count_mismatch(j.hdr_out, keep + off, n, diff, st)) == cudaSuccess)
+                    e = cudaMemcpyAsync(&d, diff, sizeof d, cudaMemcpyDeviceToHost, st);
+                mism += d;
+            }
+            if (e != cudaSuccess) break;
+            off += n;
+        }
+        if (e != cudaSuccess) { out = cuda_fail(e, "kt_batch_autotune: compare images"); break; }
+        for (uint32_t r = 0; r < reps && e == cudaSuccess; ++r) {
+            if ((e = cudaEventRecord(ev[2 * r], st)) == cudaSuccess && (e = batch_launch(b, st)) == cudaSuccess)
+                e = cudaEventRecord(ev[2 * r + 1], st);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { out = cuda_fail(e, "kt_batch_autotune: timed launches"); break; }
+        std::vector<float> ms(reps);
+        for (uint32_t r = 0; r < reps; ++r) cudaEventElapsedTime(&ms[r], ev[2 * r], ev[2 * r + 1]);
+        std::sort(ms.begin(), ms.end());
+        kt_tune_entry row;
+        row.tuning = cands[i];
+        row.ms = ms[reps / 2];
+        row.identical = mism == 0 ? 1 : 0;
+        rows.push_back(row);
+    }
+    release();
+    if (out != KT_OK) {
+        kt_batch_set_tuning(b, &saved);
+        return out;
+    }
+    size_t best = 0;
+    for (size_t i = 1; i < rows.size(); ++i)
+        if (rows[i].identical && rows[i].ms < rows[best].ms) best = i;
+    if ((out = kt_batch_set_tuning(b, &rows[best].tuning)) != KT_OK) return out;
+    if (table)
+        for (size_t i = 0; i < rows.size(); ++i) table[i] = rows[i];
+    if (n_entries) *n_entries = (uint32_t)rows.size();
     return KT_OK;
 }
 

@@ -56,13 +56,19 @@ struct BatchJob {
     uint32_t* err;
     int tiles_x;
     int tile_begin;
+    unsigned unit_begin;  // persistent launch: first 32-pixel unit of this job
 };
 struct BatchTable {
     BatchJob job[kBatchMaxJobs];
     int n;
     int total_tiles;
+    unsigned total_units;
 };
 cudaError_t launch_batch(const BatchTable& bt, int bx, int by, cudaStream_t stream);
+// Persistent batched trace: warps take 32-pixel units, each inside one job, from the device
+// counter `counter` (one word, reset here on `stream`); blocks of 128 threads, blocks_per_sm
+// resident per SM (the FP32 reference-semantics kernel has 4, 5 and 6; the others their default).
+cudaError_t launch_batch_persistent(const BatchTable& bt, int blocks_per_sm, unsigned* counter, cudaStream_t stream);
 // Number of 16-byte words that differ between a and b (n16 words each) into *out (device).
 cudaError_t launch_count_mismatch(const void* a, const void* b, size_t n16, unsigned long long* out,
                                   cudaStream_t stream);

@@ -467,6 +467,71 @@ cudaError_t launch_batch(const BatchTable& bt, int bx, int by, cudaStream_t st) 
     return launch_batch_typed<float, 0>(bt, bx, by, st);
 }
 
+// Persistent batched trace.  The pixels of every job are cut into units of 32 (the tile order of
+// unit_to_pixel, so a unit is a 16x2 patch of one frame); job j owns units [unit_begin,
+// unit_begin of j + 1).  A warp takes one unit at a time from a single device counter over all
+// jobs, so the 32 rays of a warp always share one scene and its parameters stay uniform
+// constant-bank loads, and an SM never waits for a whole block: each warp moves on as soon as
+// its own unit is done.  Per-pixel arithmetic is the plain kernel's (run_ray).
+template <class R, int MODE, int MINB>
+__global__ void __launch_bounds__(kWavefrontBlock, MINB)
+    trace_batch_persistent_kernel(const __grid_constant__ BatchTable bt, unsigned* __restrict__ counter) {
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        unsigned u = 0;
+        if (lane == 0) u = atomicAdd(counter, 1u);
+        u = __shfl_sync(kFull, u, 0);
+        if (u >= bt.total_units) break;
+        int lo = 0, hi = bt.n - 1;  // last job whose first unit is <= u
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bt.job[mid].unit_begin <= u) lo = mid; else hi = mid - 1;
+        }
+        const BatchJob& jb = bt.job[lo];
+        const Scene& sc = jb.sc;
+        const unsigned pix = (u - jb.unit_begin) * 32u + (unsigned)lane;
+        if (pix < (unsigned)sc.width * (unsigned)sc.height) {
+            int px, py;
+            unit_to_pixel(pix, sc.width, sc.height, px, py);
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+            Tally total;
+            total.clear();
+            for (int smp = 0; smp < sc.spp; ++smp)
+                run_ray<R, MODE, false>(px, py, smp, sc, jb.cam, jb.err, acc, total, nullptr);
+            const float fs = sc.final_scale;
+            jb.hdr[py * sc.width + px] = make_float4(acc[0] * fs, acc[1] * fs, acc[2] * fs, 1.0f);
+        }
+    }
+}
+
+template <class R, int MODE, int MINB>
+static cudaError_t launch_batch_persistent_minb(const BatchTable& bt, unsigned* counter, cudaStream_t st) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_batch_persistent_kernel<R, MODE, MINB>,
+                                                           kWavefrontBlock, 0)) != cudaSuccess)
+        return e;
+    if (per_sm < 1) per_sm = 1;
+    if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+    trace_batch_persistent_kernel<R, MODE, MINB><<<sms * per_sm, kWavefrontBlock, 0, st>>>(bt, counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_persistent(const BatchTable& bt, int blocks_per_sm, unsigned* counter, cudaStream_t st) {
+    if (bt.n <= 0 || bt.total_units == 0) return cudaSuccess;
+    const Scene& s0 = bt.job[0].sc;
+    if (s0.precision == 2) return launch_batch_persistent_minb<double, 1, 2>(bt, counter, st);
+    if (s0.precision == 1) return launch_batch_persistent_minb<Mixed, 1, 4>(bt, counter, st);
+    if (s0.mode == 1) return launch_batch_persistent_minb<float, 1, 4>(bt, counter, st);
+    switch (blocks_per_sm) {
+        case 5: return launch_batch_persistent_minb<float, 0, 5>(bt, counter, st);
+        case 6: return launch_batch_persistent_minb<float, 0, 6>(bt, counter, st);
+        default: return launch_batch_persistent_minb<float, 0, 4>(bt, counter, st);
+    }
+}
+
 // ---- image comparison (the autotuner's bit-identity filter) ---------------------------------
 __global__ void __launch_bounds__(256) count_mismatch_kernel(const uint4* __restrict__ a, const uint4* __restrict__ b,
                                                              size_t n, unsigned long long* __restrict__ out) {

@@ -52,6 +52,27 @@ def test_batch_matches_per_job_traces(cuda, mode, prec):
         h.fill_(-1.0)
     b.trace_sequential()
     check()
+    # the persistent launch (32-pixel units of one job per warp, one counter over all jobs)
+    for bps in (4, 6):
+        b.set_tuning(kt.SCHED_WAVEFRONT, blocks_per_sm=bps)
+        assert b.tuning().schedule == kt.SCHED_WAVEFRONT
+        for h, _ in bufs:
+            h.fill_(-1.0)
+        b.trace()
+        check()
+        for h, _ in bufs:
+            h.fill_(-1.0)
+        b.trace_graph()
+        b.trace_graph()
+        check()
+    # the batch tuner: every candidate identical, the installed one reproduces the images
+    rows = b.autotune(reps=1)
+    assert len(rows) == (9 if prec == kt.PREC_FP32 else 7) and all(ok for _, _, ok in rows)
+    for h, _ in bufs:
+        h.fill_(-1.0)
+    b.trace_graph()
+    check()
+    b.set_block(8, 8)
     # a new camera for job 2 is picked up by the next graph launch
     cfg2, _ = jobs[2]
     cam2 = kt.orbit_camera(77.0, 33.0, 25.0)
