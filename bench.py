@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-c3", action="store_true", help="skip the 4096^2 x 8-draw precision ablation")
     ap.add_argument("--no-sequence", action="store_true", help="skip the headless frame-sequence leg")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-scale", type=int, default=1,
+                    help="divide the batched workload's frame sizes by this (small cases for profiling)")
     ap.add_argument("--no-pareto", action="store_true",
                     help="skip the accuracy-against-speed sweep of FP32 / mixed / FP64 over tolerances")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -403,7 +405,7 @@ def pareto_leg(local, reference_tol: float = 1e-10, c3_size: int = 2048) -> dict
                              "hdr_frac_over_1e-3": float((rel > 1e-3).double().mean())})
                 ctx.close()
         best = {}
-        for target in (1e-4, 1e-5, 1e-6):
+        for target in (1e-4, 3e-5, 1e-5, 3e-6, 1e-6):
             best[f"p99<={target:g}"] = {}
             for pname, _ in precs:
                 ok = [x for x in rows if x["precision"] == pname and x["hdr_p99"] <= target]
@@ -582,7 +584,7 @@ def sequence_leg(cfg, tuning, local, moving: int = 60, resting: int = 30) -> dic
             "mrays_s": round(rays / wall / 1e6, 1), "first_frame_png_bytes": size if written else 0}
 
 
-def batch_leg(local, reps: int) -> dict:
+def batch_leg(local, reps: int, scale: int = 1) -> dict:
     """The batched-launch workload (64 renders: 16 each of 256^2, 512^2, 1024^2, 1920x1080 with
     random spins, inclinations, observer and disk radii): one batched launch in the shape the
     batch tuner picks (plain block shapes or the persistent launch), the same launch replayed from
@@ -593,13 +595,13 @@ def batch_leg(local, reps: int) -> dict:
     import kerrtrace_b200 as kt
     from kerrtrace_b200 import workloads
 
-    jobs = workloads.c4_jobs()
+    jobs = workloads.c4_jobs(scale=scale)
     bufs = [(torch.zeros((c.width * c.height, 4), device="cuda"), torch.zeros(2, dtype=torch.int32, device="cuda"))
             for c, _ in jobs]
     b = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(jobs, bufs)], local)
     rays = b.rays()
     stream = torch.cuda.current_stream().cuda_stream
-    out = {"jobs": len(jobs), "rays": rays}
+    out = {"jobs": len(jobs), "rays": rays, "scale": scale}
     # launch shape of the batched launch: kt_batch_autotune (plain block shapes and the persistent
     # launch of job-uniform 32-pixel units), every candidate checked bit for bit
     rows = b.autotune(reps=2, stream=stream)
@@ -857,7 +859,7 @@ def run_ours(args, rank, world, local):
     legs = [("retirement", args.no_retirement, lambda: retirement_leg(ctx, cfg, cam, stream)),
             ("precision", args.no_precision, lambda: precision_leg(cfg, cam, local, max(3, args.steps))),
             ("adjoint", args.no_adjoint, lambda: adjoint_leg(local, max(3, args.steps))),
-            ("batch", args.no_batch, lambda: batch_leg(local, 3)),
+            ("batch", args.no_batch, lambda: batch_leg(local, 3, args.batch_scale)),
             ("pareto", args.no_pareto, lambda: pareto_leg(local)),
             ("sequence", args.no_sequence, lambda: sequence_leg(cfg, ctx.tuning(), local)),
             ("c3", args.no_c3, lambda: c3_leg(local))]
