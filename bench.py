@@ -651,8 +651,9 @@ def adjoint_leg(local, reps: int, size: int = 512) -> dict:
     linear HDR between the image at the starting parameters and the target image; forward with
     step records, then the discrete adjoint (VJP) of the loss.  Per precision: forward, backward
     and adjoint Mrays/s (rays / (forward + backward)), the cost ratio, record memory and the
-    gradient; for FP64 also its agreement with central differences of the frozen-step model
-    (Richardson-extrapolated, double images, unresolvable pixels masked)."""
+    gradient, and its agreement with central differences of the frozen-step model
+    (Richardson-extrapolated, double images, unresolvable pixels masked; the FP32 records are
+    replayed in FP64 arithmetic for them)."""
     import torch
 
     import kerrtrace_b200 as kt
@@ -691,36 +692,42 @@ def adjoint_leg(local, reps: int, size: int = 512) -> dict:
              "cost_ratio": round((f_ms + b_ms) / f_ms, 2), "loss": loss, "grad": g.cpu().tolist(),
              "record_mb": round(info.record_bytes / 2**20, 2), "diff_device_mb": round(info.device_bytes / 2**20, 1),
              "overflow_rays": int(info.overflow_rays)}
-        if prec == kt.PREC_FP64:
-            th = list(workloads.C5_START)
-            eps = [1e-5, 1e-4, 1e-5, 1e-4]
-            mask = torch.zeros(n, dtype=torch.bool, device="cuda")
-            fd = []
-            for j in range(4):
-                img = {}
-                for sgn in (1, -1):
-                    for k in (1, 2):
-                        t2 = list(th)
-                        t2[j] += sgn * eps[j] / k
-                        hh = torch.zeros((n, 4), device="cuda")
-                        h64 = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
-                        fl = torch.zeros(n, dtype=torch.int32, device="cuda")
+        # central differences of the frozen-step model in double arithmetic: the FP64 records
+        # replayed as they are, the FP32 records replayed in FP64 (kt_diff_replay_fp64)
+        th = list(workloads.C5_START)
+        eps = [1e-5, 1e-4, 1e-5, 1e-4]
+        mask = torch.zeros(n, dtype=torch.bool, device="cuda")
+        fd = []
+        for j in range(4):
+            img = {}
+            for sgn in (1, -1):
+                for k in (1, 2):
+                    t2 = list(th)
+                    t2[j] += sgn * eps[j] / k
+                    hh = torch.zeros((n, 4), device="cuda")
+                    h64 = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+                    fl = torch.zeros(n, dtype=torch.int32, device="cuda")
+                    if prec == kt.PREC_FP64:
                         d.replay(t2, hh.data_ptr(), fl.data_ptr(), err.data_ptr(), hdr64_ptr=h64.data_ptr())
-                        torch.cuda.synchronize()
-                        img[(sgn, k)] = h64
-                        mask |= fl.bool()
-                f1 = (img[(1, 1)] - img[(-1, 1)]) / (2 * eps[j])
-                f2 = (img[(1, 2)] - img[(-1, 2)]) / eps[j]
-                mask |= ((f1 - f2).abs() > 1e-3 * f2.abs() + 1e-7 * f2.abs().max()).any(dim=1)
-                fd.append((4 * f2 - f1) / 3)
-            wm = w.clone()
-            wm[mask] = 0
-            d.backward(wm.data_ptr(), g.data_ptr())
-            torch.cuda.synchronize()
-            ga = g.cpu().tolist()
-            ref = [float((fd[j] * wm[:, :3].double()).sum()) for j in range(4)]
-            r["fd_check"] = {"eps": eps, "masked_pixels": int(mask.sum()), "adjoint": ga, "central_differences": ref,
-                             "rel_err": [abs(ga[j] - ref[j]) / max(abs(ref[j]), 1e-300) for j in range(4)]}
+                    else:
+                        d.replay_fp64(t2, h64.data_ptr(), fl.data_ptr(), err.data_ptr(), hh.data_ptr())
+                    torch.cuda.synchronize()
+                    img[(sgn, k)] = h64
+                    mask |= fl.bool()
+            f1 = (img[(1, 1)] - img[(-1, 1)]) / (2 * eps[j])
+            f2 = (img[(1, 2)] - img[(-1, 2)]) / eps[j]
+            mask |= ((f1 - f2).abs() > 1e-3 * f2.abs() + 1e-7 * f2.abs().max()).any(dim=1)
+            fd.append((4 * f2 - f1) / 3)
+        wm = w.clone()
+        wm[mask] = 0
+        d.backward(wm.data_ptr(), g.data_ptr())
+        torch.cuda.synchronize()
+        ga = g.cpu().tolist()
+        ref = [float((fd[j] * wm[:, :3].double()).sum()) for j in range(4)]
+        r["fd_check"] = {"eps": eps, "replay": "records as recorded" if prec == kt.PREC_FP64 else
+                         "FP32 records replayed in FP64 arithmetic", "masked_pixels": int(mask.sum()),
+                         "adjoint": ga, "central_differences": ref,
+                         "rel_err": [abs(ga[j] - ref[j]) / max(abs(ref[j]), 1e-300) for j in range(4)]}
         out[pname] = r
         d.close()
     return out

@@ -473,6 +473,13 @@ kt_status kt_diff_forward(kt_diff* d, void* stream, const kt_diff_params* theta,
 /* hdr64_out: optional (NULL), 3 doubles per pixel: the linear colour before the float store. */
 kt_status kt_diff_replay(kt_diff* d, void* stream, const kt_diff_params* theta, float* hdr_out, double* hdr64_out,
                          uint32_t* flags_out, uint32_t* err_word);
+/* The recorded step sequence at theta evaluated in double arithmetic (for an FP32 object, its
+ * FP32 records replayed in FP64; for an FP64 object, kt_diff_replay).  Central differences of
+ * hdr64_out measure the frozen-step model that the FP32 adjoint differentiates without the float
+ * rounding of its images.  hdr64_out: 3 doubles per pixel; flags_out (may be NULL) as
+ * kt_diff_replay; hdr_out: dev float[4*W*H]. */
+kt_status kt_diff_replay_fp64(kt_diff* d, void* stream, const kt_diff_params* theta, double* hdr64_out,
+                              uint32_t* flags_out, uint32_t* err_word, float* hdr_out);
 /* dl_dhdr: device float4 per pixel (w ignored); grad_out: device, 4 doubles (overwritten). */
 kt_status kt_diff_backward(kt_diff* d, void* stream, const float* dl_dhdr, double* grad_out);
 kt_status kt_diff_get_info(kt_diff* d, kt_diff_info* info);  /* synchronises with the device */

@@ -200,6 +200,8 @@ SIGNATURES = [
     ("kt_diff_replay", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtDiffParams), C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p]),
     ("kt_diff_backward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_diff_replay_fp64", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtDiffParams), C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
     ("kt_diff_get_info", C.c_int, [C.c_void_p, C.POINTER(KtDiffInfo)]),
     ("kt_diff_orbit_camera", C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(KtCamera),
                                        C.POINTER(KtCamera)]),
@@ -460,6 +462,12 @@ class Diff:
         p = self.params(theta)
         check(lib().kt_diff_replay(self.handle, C.c_void_p(stream), C.byref(p), C.c_void_p(hdr_ptr),
                                    C.c_void_p(hdr64_ptr or None), C.c_void_p(flags_ptr or None), C.c_void_p(err_ptr)))
+
+    def replay_fp64(self, theta, hdr64_ptr: int, flags_ptr: int, err_ptr: int, hdr_ptr: int, stream: int = 0):
+        """The recorded step sequence at theta in double arithmetic (FP32 records replayed in FP64)."""
+        p = self.params(theta)
+        check(lib().kt_diff_replay_fp64(self.handle, C.c_void_p(stream), C.byref(p), C.c_void_p(hdr64_ptr),
+                                        C.c_void_p(flags_ptr or None), C.c_void_p(err_ptr), C.c_void_p(hdr_ptr)))
 
     def backward(self, dl_dhdr_ptr: int, grad_ptr: int, stream: int = 0):
         check(lib().kt_diff_backward(self.handle, C.c_void_p(stream), C.c_void_p(dl_dhdr_ptr), C.c_void_p(grad_ptr)))

@@ -193,7 +193,23 @@ __device__ bool shade_eval(const R* X, R pt, R kt, const Scene& sc, const DiffLu
         v1.d[kSRo] = (R)__ldg(dl.dlut_dro + i1);
     }
     const T w = x - fl;
-    const T sampled = v0 + w * (v1 - v0);
+    T sampled = v0 + w * (v1 - v0);
+    if constexpr (!std::is_same<T, R>::value && sizeof(R) == 4) {
+        // Spin and r_out move the table's nodes and, at a fixed hit radius, the fetch coordinate;
+        // the two nearly cancel (the table samples one function of r), so these two tangents are
+        // summed in double from the double table: in float the remainder keeps few digits.
+        const double span_d = (double)val(r_out) - (double)val(r_in);
+        const double rh_d = (double)val(rh), wv = (double)val(w);
+        const double dv = __ldg(dl.lut_d + i1) - __ldg(dl.lut_d + i0);
+        const double du_drh = 1.0 / span_d;
+        const double du_da = -dl.dr_in_da * ((double)val(r_out) - rh_d) / (span_d * span_d);
+        const double du_dro = -(rh_d - (double)val(r_in)) / (span_d * span_d);
+        const double ga = dv * (double)n * (du_drh * (double)rh.d[kSA] + du_da) +
+                          (1.0 - wv) * __ldg(dl.dlut_da + i0) + wv * __ldg(dl.dlut_da + i1);
+        const double gro = dv * (double)n * du_dro + (1.0 - wv) * __ldg(dl.dlut_dro + i0) + wv * __ldg(dl.dlut_dro + i1);
+        sampled.d[kSA] = (R)ga;
+        sampled.d[kSRo] = (R)gro;
+    }
     const T ts = with_tangent<T>((R)sc.temp_scale, kSTs, (R)dl.dtemp_ds);
     const T T_ = ts * sampled * g;
     if (!(Ops<R>::isfiniter(val(T_)) && val(T_) > R(0))) return false;
@@ -386,7 +402,8 @@ __device__ __forceinline__ R rk_a(int m, int j) {
 // ---- forward: record / replay ----------------------------------------------------------------
 // Four resident 128-thread blocks per SM: 128 registers at most (the FP64 kernel spills about
 // 400 B there; 192 registers and two blocks otherwise).
-template <class R, bool REPLAY>
+// RR: arithmetic type of the records (R, or float records replayed in double arithmetic).
+template <class R, bool REPLAY, class RR = R>
 __global__ void __launch_bounds__(128, 4) diff_forward_kernel(const Scene sc, const Camera cam, const CameraD camd,
                                                           const DiffRecRaw rec, float4* __restrict__ hdr,
                                                           double* __restrict__ hdr64, uint32_t* __restrict__ err,
@@ -471,10 +488,10 @@ __global__ void __launch_bounds__(128, 4) diff_forward_kernel(const Scene sc, co
         if (started != (rr.term != kTermNotStarted)) flip = 1;
         if (started && rr.term != kTermNotStarted && rr.term != kTermOverflow) {
             bool done = false;
-            for (int si = rr.first_seg; si >= 0 && !done; si = seg_at<R>(rec, si)->next) {
-                const DiffSeg<R>* sg = seg_at<R>(rec, si);
+            for (int si = rr.first_seg; si >= 0 && !done; si = seg_at<RR>(rec, si)->next) {
+                const DiffSeg<RR>* sg = seg_at<RR>(rec, si);
                 for (int j = 0; j < sg->n && !done; ++j) {
-                    ry.h = sg->h[j];
+                    ry.h = (R)sg->h[j];
                     done = advance<1, true>(ry, sc, err, tl);  // one attempt: always a commit
                     ++n_done;
                 }
@@ -781,11 +798,14 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
 // ---- launchers ----------------------------------------------------------------------------------
 cudaError_t launch_diff_forward(const Scene& sc, const Camera& cam, const CameraD& camd, const DiffRecRaw& rec,
                                 int replay, float4* hdr, double* hdr64, uint32_t* err, uint32_t* flags,
-                                cudaStream_t st) {
+                                cudaStream_t st, bool float_records) {
     const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
     if (n == 0) return cudaSuccess;
     const dim3 grid((n + 127) / 128);
-    if (sc.precision == 2) {
+    if (sc.precision == 2 && float_records) {
+        if (!replay) return cudaErrorInvalidValue;
+        diff_forward_kernel<double, true, float><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
+    } else if (sc.precision == 2) {
         if (replay) diff_forward_kernel<double, true><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
         else diff_forward_kernel<double, false><<<grid, 128, 0, st>>>(sc, cam, camd, rec, hdr, hdr64, err, flags);
     } else {

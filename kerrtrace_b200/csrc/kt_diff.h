@@ -55,6 +55,7 @@ struct DiffRecRaw {
 
 // Derivatives of the scene inputs that depend on the parameters.
 struct DiffLut {
+    const double* lut_d;     // the disk LUT entries in double
     const double* dlut_da;   // d(disk LUT entry)/d(spin)
     const double* dlut_dro;  // d(disk LUT entry)/d(disk outer radius)
     double dr_in_da;         // d(ISCO)/d(spin)
@@ -72,10 +73,11 @@ struct CameraD {
 // written; replay = 1: the recorded steps at the scene's (new) parameters, flags[p] = 1 where
 // the ray's events (termination step or kind, shaded crossings) differ from the record.
 // sc.precision selects float (0) or double (2) arithmetic.  hdr64: optional, 3 doubles per
-// pixel (the colour before the float store).
+// pixel (the colour before the float store).  float_records (replay with double arithmetic
+// only): the records are DiffSeg<float>, replayed in double.
 cudaError_t launch_diff_forward(const Scene& sc, const Camera& cam, const CameraD& camd, const DiffRecRaw& rec,
                                 int replay, float4* hdr, double* hdr64, uint32_t* err, uint32_t* flags,
-                                cudaStream_t stream);
+                                cudaStream_t stream, bool float_records = false);
 // Scratch of the adjoint's work ordering: bucket and order (one word per pixel each), ctl
 // (kDiffWorkCtl words).
 constexpr int kDiffWorkCtl = 65;

@@ -213,11 +213,12 @@ void destroy(kt_diff* d) {
 // fields come from the float configuration at theta (the renderer's scene); the FP64 path also
 // gets theta in double: spin, disk radii, temperature scale, camera and a double disk LUT.
 kt_status prepare(kt_diff* d, const kt_diff_params* th, kt_diff_luts& luts, cudaStream_t st, ktd::Scene* sc,
-                  ktd::Camera* cam, ktd::CameraD* camd, ktd::CameraD* dcamd, ktd::DiffLut* dl) {
+                  ktd::Camera* cam, ktd::CameraD* camd, ktd::CameraD* dcamd, ktd::DiffLut* dl, bool force64 = false) {
     if (!std::isfinite(th->spin) || !std::isfinite(th->inclination_deg) || !std::isfinite(th->temperature_scale) ||
         !std::isfinite(th->disk_outer_radius))
         return err_arg("diff parameters must be finite");
     kt_config c = d->cfg;
+    if (force64) c.precision = KT_PREC_FP64;
     c.spin = (float)th->spin;
     c.disk_outer_radius = (float)th->disk_outer_radius;
     c.disk_temperature_scale = (float)((double)d->view.base_temperature_scale * th->temperature_scale);
@@ -272,6 +273,7 @@ kt_status prepare(kt_diff* d, const kt_diff_params* th, kt_diff_luts& luts, cuda
     kt_camera hc, hd;
     orbit_camera(d->view.observer_r, th->inclination_deg, d->view.azimuth_deg, d->view.fov_deg, &hc, &hd, camd, dcamd);
     *cam = to_dev_camera(hc);
+    dl->lut_d = luts.disk_d;
     dl->dlut_da = luts.dlut_da;
     dl->dlut_dro = luts.dlut_dro;
     dl->dr_in_da = r_in.d[0];
@@ -400,6 +402,26 @@ kt_status kt_diff_replay(kt_diff* d, void* stream, const kt_diff_params* theta, 
     const cudaError_t e = ktd::launch_diff_forward(sc, cam, camd, record_of(d), 1, reinterpret_cast<float4*>(hdr_out),
                                                    hdr64_out, err_word, flags_out, st);
     if (e != cudaSuccess) return err_cuda(e, "diff replay launch");
+    return KT_OK;
+}
+
+kt_status kt_diff_replay_fp64(kt_diff* d, void* stream, const kt_diff_params* theta, double* hdr64_out,
+                              uint32_t* flags_out, uint32_t* err_word, float* hdr_out) {
+    if (!d || !theta || !hdr64_out || !err_word || !hdr_out) return err_arg("NULL argument");
+    if (!d->have_record) return ktd::set_error(KT_ERR_NOT_READY, "kt_diff_replay_fp64 needs a kt_diff_forward first");
+    DevGuard g(d->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    ktd::Scene sc;
+    ktd::Camera cam;
+    ktd::CameraD camd, dcamd;
+    ktd::DiffLut dl;
+    kt_status s = prepare(d, theta, d->lut_rep, st, &sc, &cam, &camd, &dcamd, &dl, true);
+    if (s != KT_OK) return s;
+    sc.max_attempts = 1;
+    const bool float_records = d->cfg.precision == KT_PREC_FP32;
+    const cudaError_t e = ktd::launch_diff_forward(sc, cam, camd, record_of(d), 1, reinterpret_cast<float4*>(hdr_out),
+                                                   hdr64_out, err_word, flags_out, st, float_records);
+    if (e != cudaSuccess) return err_cuda(e, "diff FP64 replay launch");
     return KT_OK;
 }
 
