@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--size", default=None, help="WxH override of the scene resolution (same scene otherwise)")
+    ap.add_argument("--tuning", default=None,
+                    help="schedule,block_x,block_y,blocks_per_sm,refill_min,order: this launch shape instead of "
+                         "the autotuner's (reproducible profiling)")
     return ap.parse_args()
 
 
@@ -755,7 +758,13 @@ def run_ours(args, rank, world, local):
         measured_fma = kt.fma_peak(local, 16384)
     except kt.KtError:
         measured_fma = None
-    tuned = autotune.autotune(ctx, cam, stream=stream) if sched == kt.SCHED_AUTO else None
+    if args.tuning:
+        sc_, bx_, by_, bps_, rf_, od_ = (int(v) for v in args.tuning.split(","))
+        ctx.set_tuning(schedule=sc_, block_x=bx_, block_y=by_, blocks_per_sm=bps_, refill_min=rf_, order=od_)
+        sched = kt.SCHED_AUTO
+        tuned = None
+    else:
+        tuned = autotune.autotune(ctx, cam, stream=stream) if sched == kt.SCHED_AUTO else None
     stats = ctx.trace_counted(cam, hdr.data_ptr(), err.data_ptr(), stream, sched)
     work = flops.trace_flops(stats)
 
