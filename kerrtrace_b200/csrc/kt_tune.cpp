@@ -110,6 +110,15 @@ extern "C" kt_status kt_context_autotune(kt_context* ctx, void* stream, const kt
         }
     } restore{ctx->device, prev_dev};
 
+    // any failure below puts the caller's tuning back
+    struct KeepTuning {
+        kt_context* ctx;
+        kt_tuning saved;
+        bool done = false;
+        ~KeepTuning() {
+            if (!done) kt_context_set_tuning(ctx, &saved);
+        }
+    } keep{ctx, saved};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t px = (size_t)ctx->cfg.width * ctx->cfg.height;
     Scratch sc;
@@ -126,15 +135,9 @@ extern "C" kt_status kt_context_autotune(kt_context* ctx, void* stream, const kt
     std::vector<kt_tune_entry> rows;
     rows.reserve(cands.size());
     for (size_t i = 0; i < cands.size(); ++i) {
-        if ((st = kt_context_set_tuning(ctx, &cands[i])) != KT_OK) {
-            kt_context_set_tuning(ctx, &saved);
-            return st;
-        }
+        if ((st = kt_context_set_tuning(ctx, &cands[i])) != KT_OK) return st;
         if ((e = cudaMemsetAsync(sc.err, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return tune_fail(e, "clear error word");
-        if ((st = kt_trace(ctx, stream, cam, KT_SCHED_AUTO, sc.hdr, sc.err)) != KT_OK) {
-            kt_context_set_tuning(ctx, &saved);
-            return st;
-        }
+        if ((st = kt_trace(ctx, stream, cam, KT_SCHED_AUTO, sc.hdr, sc.err)) != KT_OK) return st;
         unsigned long long diff = 0;
         if (i == 0) {
             if ((e = cudaMemcpyAsync(sc.base, sc.hdr, px * 4 * sizeof(float), cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
@@ -146,10 +149,7 @@ extern "C" kt_status kt_context_autotune(kt_context* ctx, void* stream, const kt
         }
         for (uint32_t r = 0; r < reps; ++r) {
             if ((e = cudaEventRecord(sc.ev[2 * r], s)) != cudaSuccess) return tune_fail(e, "record event");
-            if ((st = kt_trace(ctx, stream, cam, KT_SCHED_AUTO, sc.hdr, sc.err)) != KT_OK) {
-                kt_context_set_tuning(ctx, &saved);
-                return st;
-            }
+            if ((st = kt_trace(ctx, stream, cam, KT_SCHED_AUTO, sc.hdr, sc.err)) != KT_OK) return st;
             if ((e = cudaEventRecord(sc.ev[2 * r + 1], s)) != cudaSuccess) return tune_fail(e, "record event");
         }
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return tune_fail(e, "synchronise");
@@ -169,6 +169,7 @@ extern "C" kt_status kt_context_autotune(kt_context* ctx, void* stream, const kt
         if (rows[i].identical && (best == rows.size() || rows[i].ms < rows[best].ms)) best = i;
     // the first candidate is identical to itself, so best is always found
     if ((st = kt_context_set_tuning(ctx, &rows[best].tuning)) != KT_OK) return st;
+    keep.done = true;
     if (table)
         for (size_t i = 0; i < rows.size(); ++i) table[i] = rows[i];
     if (n_entries) *n_entries = (uint32_t)rows.size();
