@@ -341,10 +341,11 @@ __device__ __forceinline__ void start_dual(int px, int py, const Scene& sc, cons
 // Stages of one DP5 step from s with step h (ray_advance's expressions): k[0..6] = k1..k7,
 // nx = the 5th-order state.
 template <class R>
-__device__ __forceinline__ void dp5_stages(const R* s, R h, R pt, R a, R aa, R M, R (*k)[6], R* nx) {
+__device__ __forceinline__ void dp5_stages(const R* s, R h, R pt, R a, R aa, R M, R (*k)[6], R* nx,
+                                           bool k1_given = false) {
     using C = DP<R>;
     R y[6];
-    hamilton_rhs<R, true>(s, pt, a, aa, M, k[0]);
+    if (!k1_given) hamilton_rhs<R, true>(s, pt, a, aa, M, k[0]);
 #pragma unroll
     for (int c = 0; c < 6; ++c) y[c] = s[c] + h * C::a21 * k[0][c];
     hamilton_rhs<R, true>(y, pt, a, aa, M, k[1]);
@@ -597,8 +598,10 @@ __device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], 
     return t;
 }
 
-// Resident 128-thread blocks per SM asked of the compiler for the adjoint kernel.
-template <class R> struct BackMinBlocks { static constexpr int v = 4; };
+// Resident 128-thread blocks per SM asked of the compiler for the adjoint kernel: two, so that the
+// reverse sweep's dual-number right-hand sides keep their values in registers (225 registers,
+// no spills; four blocks per SM cap them at 128 with 452 B of spills and run 14% slower).
+template <class R> struct BackMinBlocks { static constexpr int v = 2; };
 template <> struct BackMinBlocks<double> { static constexpr int v = 2; };
 
 template <class R>
@@ -651,7 +654,12 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
                         R nx[6];
 #pragma unroll
                         for (int c = 0; c < 6; ++c) S[j][c] = s[c];
-                        dp5_stages<R>(s, sg->h[j], pt, a, aa, M, K[j], nx);
+                        // FSAL: the previous step's k7 is f at this step's start, bit for bit
+                        if (j > 0) {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) K[j][0][c] = K[j - 1][6][c];
+                        }
+                        dp5_stages<R>(s, sg->h[j], pt, a, aa, M, K[j], nx, j > 0);
                         if (hits >> j & 1u) {
                             R X[6], c3[3], al;
                             step_hit<R>(s, nx, K[j], sg->h[j], X, nullptr);
