@@ -225,6 +225,12 @@ kt_status kt_context_create(const kt_config* cfg, int device, kt_context** out);
 /* Same, with caller-supplied LUTs (host arrays: bb_rgba lut_n*4 floats, disk lut_n floats). */
 kt_status kt_context_create_with_luts(const kt_config* cfg, int device, const float* bb_rgba,
                                       const float* disk, uint32_t lut_n, kt_context** out);
+/* Same as kt_context_create, with both LUTs generated on the device (kt_generate_*_lut_device)
+ * and the textures filled from device memory: no host table is built or copied.  The device
+ * tables agree with the host's (which are bit-equal to the reference's Rust generators) to a few
+ * ulp, so images match kt_context_create's to the parity tolerance, not bit for bit.
+ * Synchronises the device once. */
+kt_status kt_context_create_device_luts(const kt_config* cfg, int device, kt_context** out);
 void kt_context_destroy(kt_context* ctx);
 /* Copies out the derived KerrParams the context uses. */
 kt_status kt_context_params(const kt_context* ctx, kt_kerr_params* out);

@@ -176,6 +176,7 @@ SIGNATURES = [
     ("kt_context_create", C.c_int, [C.POINTER(KtConfig), C.c_int, C.POINTER(C.c_void_p)]),
     ("kt_context_create_with_luts", C.c_int, [C.POINTER(KtConfig), C.c_int, C.c_void_p, C.c_void_p, C.c_uint32,
                                               C.POINTER(C.c_void_p)]),
+    ("kt_context_create_device_luts", C.c_int, [C.POINTER(KtConfig), C.c_int, C.POINTER(C.c_void_p)]),
     ("kt_context_destroy", None, [C.c_void_p]),
     ("kt_context_params", C.c_int, [C.c_void_p, C.POINTER(KtKerrParams)]),
     ("kt_trace", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtCamera), C.c_int32, C.c_void_p, C.c_void_p]),
@@ -362,9 +363,13 @@ class Context:
     `c_params` upload and texture creation, src/renderer/init.rs:74-140)."""
 
     def __init__(self, cfg: KtConfig, device: int = 0, luts=None):
+        """luts: None (host tables, the reference's), "device" (tables generated on the device) or
+        a pair of arrays (blackbody rows, disk table)."""
         self.cfg = cfg.copy()
         h = C.c_void_p()
-        if luts is None:
+        if isinstance(luts, str) and luts == "device":
+            check(lib().kt_context_create_device_luts(C.byref(self.cfg), device, C.byref(h)))
+        elif luts is None:
             check(lib().kt_context_create(C.byref(self.cfg), device, C.byref(h)))
         else:
             import numpy as np

@@ -478,14 +478,14 @@ void destroy_ctx(kt_context* c) {
 // channels, linear filtering, normalised coordinates, clamp addressing.  The blackbody LUT is
 // allocated with height 1, the disk LUT with height 0, as in texture.rs:37-67.
 kt_status make_lut_texture(const float* host, uint32_t n, int channels, size_t height,
-                           cudaArray_t* arr, cudaTextureObject_t* tex) {
+                           cudaArray_t* arr, cudaTextureObject_t* tex,
+                           cudaMemcpyKind kind = cudaMemcpyHostToDevice) {
     const cudaChannelFormatDesc desc =
         channels == 4 ? cudaCreateChannelDesc(32, 32, 32, 32, cudaChannelFormatKindFloat)
                       : cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
     KT_CUDA(cudaMallocArray(arr, &desc, n, height, cudaArrayDefault), "cudaMallocArray");
     const size_t row_bytes = (size_t)n * channels * sizeof(float);
-    KT_CUDA(cudaMemcpy2DToArray(*arr, 0, 0, host, row_bytes, row_bytes, 1, cudaMemcpyHostToDevice),
-            "copy LUT to CUDA array");
+    KT_CUDA(cudaMemcpy2DToArray(*arr, 0, 0, host, row_bytes, row_bytes, 1, kind), "copy LUT to CUDA array");
     cudaResourceDesc rd;
     std::memset(&rd, 0, sizeof rd);
     rd.resType = cudaResourceTypeArray;
@@ -618,8 +618,10 @@ kt_status validate_cfg(const kt_config* cfg) {
     return KT_OK;
 }
 
+// device_luts: both tables are generated on the device (kt_generate_*_lut_device, on the legacy
+// default stream) and the textures are filled from there.
 kt_status create_impl(const kt_config* cfg, int device, const float* bb_in, const float* disk_in,
-                      uint32_t lut_n, kt_context** out) {
+                      uint32_t lut_n, kt_context** out, bool device_luts = false) {
     if (!out) return fail(KT_ERR_INVALID_ARG, "out is NULL");
     *out = nullptr;
     kt_status st = validate_cfg(cfg);
@@ -642,7 +644,7 @@ kt_status create_impl(const kt_config* cfg, int device, const float* bb_in, cons
         if (lut_n != n) return bail(fail(KT_ERR_INVALID_ARG, "LUT length %u does not match lut_size %u", lut_n, n));
         bb.assign(bb_in, bb_in + 4 * (size_t)n);
         disk.assign(disk_in, disk_in + n);
-    } else {
+    } else if (!device_luts) {
         bb.resize(4 * (size_t)n);
         disk.resize(n);
         if ((st = kt_generate_blackbody_lut(n, cfg->lut_max_temp, cfg->wavelength_start, cfg->wavelength_end,
@@ -654,17 +656,36 @@ kt_status create_impl(const kt_config* cfg, int device, const float* bb_in, cons
     cudaGetDevice(&prev);
     if (cudaSetDevice(device) != cudaSuccess) return bail(fail(KT_ERR_CUDA, "cudaSetDevice(%d) failed", device));
     auto step = [&](kt_status s) { if (s != KT_OK) { cudaSetDevice(prev); destroy_ctx(c); } return s; };
-    if ((st = step(make_lut_texture(bb.data(), n, 4, 1, &c->bb_array, &c->bb_tex))) != KT_OK) return st;
-    if ((st = step(make_lut_texture(disk.data(), n, 1, 0, &c->disk_array, &c->disk_tex))) != KT_OK) return st;
     cudaError_t e;
-    if ((e = cudaMalloc(&c->bb_lut_dev, bb.size() * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&c->disk_lut_dev, disk.size() * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&c->queue, 64)) != cudaSuccess ||
+    if ((e = cudaMalloc(&c->bb_lut_dev, 4 * (size_t)n * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->disk_lut_dev, (size_t)n * sizeof(float))) != cudaSuccess)
+        return step(cuda_fail(e, "context LUT allocation"));
+    if (device_luts) {
+        if ((st = step(kt_generate_blackbody_lut_device(n, cfg->lut_max_temp, cfg->wavelength_start, cfg->wavelength_end,
+                                                        cfg->wavelength_step, reinterpret_cast<float*>(c->bb_lut_dev),
+                                                        nullptr))) != KT_OK ||
+            (st = step(kt_generate_disk_lut_device(&c->params, cfg->disk_outer_radius, n, c->disk_lut_dev, nullptr))) !=
+                KT_OK)
+            return st;
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return step(cuda_fail(e, "device LUT generation"));
+        const float* bbd = reinterpret_cast<const float*>(c->bb_lut_dev);
+        if ((st = step(make_lut_texture(bbd, n, 4, 1, &c->bb_array, &c->bb_tex, cudaMemcpyDeviceToDevice))) != KT_OK)
+            return st;
+        if ((st = step(make_lut_texture(c->disk_lut_dev, n, 1, 0, &c->disk_array, &c->disk_tex, cudaMemcpyDeviceToDevice))) !=
+            KT_OK)
+            return st;
+    } else {
+        if ((st = step(make_lut_texture(bb.data(), n, 4, 1, &c->bb_array, &c->bb_tex))) != KT_OK) return st;
+        if ((st = step(make_lut_texture(disk.data(), n, 1, 0, &c->disk_array, &c->disk_tex))) != KT_OK) return st;
+        if ((e = cudaMemcpy(c->bb_lut_dev, bb.data(), bb.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(c->disk_lut_dev, disk.data(), disk.size() * sizeof(float), cudaMemcpyHostToDevice)) !=
+                cudaSuccess)
+            return step(cuda_fail(e, "LUT upload"));
+    }
+    if ((e = cudaMalloc(&c->queue, 64)) != cudaSuccess ||
         (e = cudaMalloc(&c->counters, 8 * sizeof(unsigned long long))) != cudaSuccess ||
         (c->post.active &&
-         (e = cudaMalloc(&c->bloom_scratch, (size_t)cfg->width * cfg->height * sizeof(float4))) != cudaSuccess) ||
-        (e = cudaMemcpy(c->bb_lut_dev, bb.data(), bb.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(c->disk_lut_dev, disk.data(), disk.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+         (e = cudaMalloc(&c->bloom_scratch, (size_t)cfg->width * cfg->height * sizeof(float4))) != cudaSuccess))
         return step(cuda_fail(e, "context allocation"));
     if ((st = step(fill_scene(c))) != KT_OK) return st;
     cudaSetDevice(prev);
@@ -723,6 +744,9 @@ extern "C" {
 
 kt_status kt_context_create(const kt_config* cfg, int device, kt_context** out) {
     return create_impl(cfg, device, nullptr, nullptr, 0, out);
+}
+kt_status kt_context_create_device_luts(const kt_config* cfg, int device, kt_context** out) {
+    return create_impl(cfg, device, nullptr, nullptr, 0, out, true);
 }
 kt_status kt_context_create_with_luts(const kt_config* cfg, int device, const float* bb_rgba,
                                       const float* disk, uint32_t lut_n, kt_context** out) {

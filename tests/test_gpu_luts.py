@@ -38,3 +38,37 @@ def test_device_luts_match_host_luts(cuda, name):
     # of either libm grows to 1.7e-5 of the table maximum there
     assert rel_disk < 1e-4, rel_disk
     assert dev_disk[0] == 0.0 and host_disk[0] == 0.0
+
+
+@pytest.mark.parametrize("name,size", [("c2", (320, 180)), ("t1", None), ("c1", (128, 128))])
+def test_context_with_device_luts_renders_within_parity(cuda, name, size):
+    """A context whose LUTs were generated on the device (kt_context_create_device_luts) renders
+    the frame of a host-table context to the parity tolerance, and its post gives the same image
+    to one code value."""
+    from tests.helpers import compare_hdr, run_ours
+    cfg, cam = workloads.scene(name)
+    if size:
+        cfg = workloads.scaled(cfg, *size)
+    a, ea, _, ca = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN)
+    cd = kt.Context(cfg, luts="device")
+    b, eb, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_PLAIN, ctx=cd)
+    r = compare_hdr(b, a, cfg.width, cfg.height)
+    print(name, r)
+    assert np.all(b[:, 3] == 1.0)
+    assert r["class_mismatch_inner"] == 0, r
+    assert r["over_tol_inner"] <= max(2, 2e-4 * r["n"]), r
+    assert r["over_tol_all"] <= max(2, 0.005 * r["n"]), r
+    assert np.array_equal(ea, eb)
+    n = cfg.width * cfg.height
+    img = {}
+    for key, ctx, h in (("host", ca, a), ("device", cd, b)):
+        hd = cuda.tensor(h, device="cuda")
+        im = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+        ctx.post_fused(hd.data_ptr(), im.data_ptr())
+        cuda.cuda.synchronize()
+        img[key] = im.cpu().numpy().view(np.uint32)
+    d = np.max(np.abs(np.stack([(img["host"] >> s) & 255 for s in (16, 8, 0)]).astype(int) -
+                      np.stack([(img["device"] >> s) & 255 for s in (16, 8, 0)]).astype(int)), axis=0)
+    assert np.mean(d > 1) <= 1e-3, np.bincount(d)
+    ca.close()
+    cd.close()
