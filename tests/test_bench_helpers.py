@@ -28,3 +28,15 @@ def test_histogram_quantiles_are_within_one_bin():
     bench._log_hist(torch.zeros(10, dtype=torch.float64), hz)
     assert float(hz[0]) == 10
     assert bench._hist_quantile(torch.zeros(1300, dtype=torch.float64), 0.5) is None
+
+
+def test_both_arms_describe_the_same_workload(kt, orc):
+    """bench.py's own arm builds its scene through the library's host entry points, the
+    reference arm through the oracle's restatement (so that it loads no product library); both
+    must print the same config.workload and see the same scene and camera bits."""
+    from kerrtrace_b200 import workloads
+    for size in (None, "480x270"):
+        c_lib, cam_lib = bench.rank_camera(workloads, "c2", 0, 1, size)
+        c_ref, cam_ref = bench.rank_camera(workloads, "c2", 0, 1, size, host=orc.Host())
+        assert bench.workload_label("c2", c_lib) == bench.workload_label("c2", c_ref)
+        assert bytes(c_lib) == bytes(c_ref) and bytes(cam_lib) == bytes(cam_ref)
