@@ -341,7 +341,8 @@ __device__ __forceinline__ void start_dual(int px, int py, const Scene& sc, cons
 // Stages of one DP5 step from s with step h (ray_advance's expressions): k[0..6] = k1..k7,
 // nx = the 5th-order state.
 template <class R>
-__device__ __forceinline__ void dp5_stages(const R* s, R h, R pt, R a, R aa, R M, R (*k)[6], R* nx,
+// Stages k1..k6 into k, the 5th-order state into nx and k7 = f(nx) into k7.
+__device__ __forceinline__ void dp5_stages(const R* s, R h, R pt, R a, R aa, R M, R (*k)[6], R* nx, R* k7,
                                            bool k1_given = false) {
     using C = DP<R>;
     R y[6];
@@ -368,7 +369,7 @@ __device__ __forceinline__ void dp5_stages(const R* s, R h, R pt, R a, R aa, R M
     for (int c = 0; c < 6; ++c)
         nx[c] = s[c] + h * (C::b1 * k[0][c] + C::b3 * k[2][c] + C::b4 * k[3][c] + C::b5 * k[4][c] +
                             C::b6 * k[5][c]);
-    hamilton_rhs<R, true>(nx, pt, a, aa, M, k[6]);
+    hamilton_rhs<R, true>(nx, pt, a, aa, M, k7);
 }
 
 // Runge-Kutta matrix with row 7 = b (the stage-7 input is the 5th-order state).
@@ -584,16 +585,16 @@ __global__ void __launch_bounds__(256) diff_bucket_scatter_kernel(unsigned n, co
 // Hit point of step (s -> nx) with stages k: the crossing root of shade_crossing<R, 1>; X the
 // state there, dX its slope in the step fraction.
 template <class R>
-__device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], R h, R* X, R* dX) {
+__device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], const R* k7, R h, R* X, R* dX) {
     const R yv0 = s[1], yv1 = nx[1];
     const R dy = yv0 - yv1;
     R t = dy != R(0) ? Ops<R>::fdiv(yv0, dy) : R(0.5);
     t = Ops<R>::minr(Ops<R>::maxr(t, R(0)), R(1));
-    t = crossing_root<R>(yv0, yv1, k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1], h, t);
+    t = crossing_root<R>(yv0, yv1, k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k7[1], h, t);
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
-        X[c] = dense_eval<R>(s[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c], h, t);
-        if (dX) dX[c] = dense_slope<R>(s[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k[6][c], h, t);
+        X[c] = dense_eval<R>(s[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k7[c], h, t);
+        if (dX) dX[c] = dense_slope<R>(s[c], nx[c], k[0][c], k[2][c], k[3][c], k[4][c], k[5][c], k7[c], h, t);
     }
     return t;
 }
@@ -633,7 +634,8 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
             R lpt = R(0), lkt = R(0), ga = R(0), gts = R(0), gro = R(0);
             R ltau = rr.term == kTermEscape ? (lc[0] + lc[1] + lc[2]) * (R)rr.sky : R(0);
             R S[kSegSteps][6];          // state before each step of the segment
-            R K[kSegSteps][7][6];       // its stages
+            R K[kSegSteps][6][6];       // its stages k1..k6 (a step's k7 is the next step's k1)
+            R K7[6];                    // k7 of the segment's last step
             R TIN[kSegSteps];           // transmittance before a shaded crossing
             // the adjoint of the state is zero after the last shaded crossing: start there
             int si = rr.last_seg;
@@ -657,12 +659,12 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
                         // FSAL: the previous step's k7 is f at this step's start, bit for bit
                         if (j > 0) {
 #pragma unroll
-                            for (int c = 0; c < 6; ++c) K[j][0][c] = K[j - 1][6][c];
+                            for (int c = 0; c < 6; ++c) K[j][0][c] = K7[c];
                         }
-                        dp5_stages<R>(s, sg->h[j], pt, a, aa, M, K[j], nx, j > 0);
+                        dp5_stages<R>(s, sg->h[j], pt, a, aa, M, K[j], nx, K7, j > 0);
                         if (hits >> j & 1u) {
                             R X[6], c3[3], al;
-                            step_hit<R>(s, nx, K[j], sg->h[j], X, nullptr);
+                            step_hit<R>(s, nx, K[j], K7, sg->h[j], X, nullptr);
                             TIN[j] = tau;
                             if (shade_eval<R, R>(X, pt, kt, sc, dl, c3, al)) tau *= R(1) - al;
                         }
@@ -674,6 +676,7 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
                 for (int j = n - 1; j >= 0; --j) {
                     const R h = sg->h[j];
                     const R(*k)[6] = K[j];
+                    const R* k7 = j + 1 < n ? K[j + 1][0] : K7;
                     const R* s0 = S[j];
                     R nx[6];
 #pragma unroll
@@ -689,7 +692,7 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
                         for (int c = 0; c < 6; ++c) dk[i][c] = R(0);
                     if (hits >> j & 1u) {
                         R X[6], dX[6];
-                        const R t = step_hit<R>(s0, nx, k, h, X, dX);
+                        const R t = step_hit<R>(s0, nx, k, k7, h, X, dX);
                         Dual<R, kSN> cc[3], al;
                         if (shade_eval<R, Dual<R, kSN>>(X, pt, kt, sc, dl, cc, al)) {
                             const R tin = TIN[j];
