@@ -96,3 +96,38 @@ def test_batch_limits(cuda):
     c2.mode = kt.MODE_SPEC
     with pytest.raises(kt.KtError):
         kt.Batch([(cfg, cam, h.data_ptr(), e.data_ptr()), (c2, cam, h.data_ptr(), e.data_ptr())])
+
+
+@pytest.mark.parametrize("schedule", [kt.SCHED_PLAIN, kt.SCHED_WAVEFRONT])
+def test_batch_jobs_match_the_reference_kernel(cuda, schedule):
+    """Jobs of one batch, compared one by one with the reference's own trace_kernel
+    (oracle/_ref).  The reference bakes some scene values into #defines, so the jobs keep the
+    1080p scene's (temperature scale, horizon epsilon, tolerance, step budget) and vary what it
+    takes at run time: spin, camera, frame size, disk outer radius and LUT range.  Plain and
+    persistent batched launches."""
+    from tests.helpers import run_ref
+    base, _ = workloads.scene("c2")
+    rng = np.random.default_rng(5)
+    jobs = []
+    for w, h in ((96, 64), (160, 90), (64, 128), (200, 120)):
+        c = workloads.scaled(base, w, h)
+        c.spin = float(rng.uniform(-0.95, 0.95))
+        c.disk_outer_radius = float(rng.uniform(12.0, 40.0))
+        c.lut_max_temp = float(rng.uniform(1e5, 3e5))
+        cam = kt.orbit_camera(float(rng.uniform(40.0, 150.0)), float(rng.uniform(10.0, 85.0)), 25.0)
+        jobs.append((c, cam))
+    bufs = _alloc(cuda, jobs)
+    b = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(jobs, bufs)])
+    if schedule == kt.SCHED_WAVEFRONT:
+        b.set_tuning(kt.SCHED_WAVEFRONT, blocks_per_sm=5)
+    else:
+        b.set_block(8, 16)
+    b.trace()
+    cuda.cuda.synchronize()
+    for (c, cam), (h, e) in zip(jobs, bufs):
+        ref, err_r = run_ref(cuda, "c2", c, cam)
+        ours = h.cpu().numpy()
+        assert np.all(ours[:, 3] == 1.0)
+        assert np.array_equal(ours.view(np.uint32), ref.view(np.uint32)), (c.width, c.height, c.spin)
+        assert np.array_equal(e.cpu().numpy().view(np.uint32), err_r)
+    b.close()
