@@ -131,3 +131,34 @@ def test_batch_jobs_match_the_reference_kernel(cuda, schedule):
         assert np.array_equal(ours.view(np.uint32), ref.view(np.uint32)), (c.width, c.height, c.spin)
         assert np.array_equal(e.cpu().numpy().view(np.uint32), err_r)
     b.close()
+
+
+def test_persistent_batch_of_64_ragged_jobs(cuda):
+    """The largest batch (64 jobs) of ragged frames, one pixel, single rows and columns and odd
+    sizes, whose 32-pixel units end inside a row or straddle none: every job equals its own
+    kt_trace bit for bit under the persistent launch (4 and 6 resident blocks per SM) and its
+    graph replay, and every pixel is written."""
+    base, _ = workloads.scene("t1")
+    sizes = [(1, 1), (1, 17), (23, 1), (37, 23), (31, 1), (33, 2), (5, 7), (64, 3)] * 8
+    rng = np.random.default_rng(9)
+    jobs = []
+    for w, h in sizes:
+        c = workloads.scaled(base, w, h)
+        c.spin = float(rng.uniform(-0.9, 0.9))
+        c.disk_temperature_scale = base.disk_temperature_scale
+        jobs.append((c, kt.orbit_camera(float(rng.uniform(20.0, 60.0)), float(rng.uniform(20.0, 85.0)), 40.0)))
+    assert len(jobs) == kt.BATCH_MAX_JOBS
+    bufs = _alloc(cuda, jobs)
+    b = kt.Batch([(c, cam, h.data_ptr(), e.data_ptr()) for (c, cam), (h, e) in zip(jobs, bufs)])
+    expected = [run_ours(cuda, c, cam, kt.SCHED_PLAIN)[0] for c, cam in jobs]
+    for bps, graph in ((4, False), (6, True)):
+        for h, _ in bufs:
+            h.fill_(-1.0)
+        b.set_tuning(kt.SCHED_WAVEFRONT, blocks_per_sm=bps)
+        (b.trace_graph if graph else b.trace)()
+        cuda.cuda.synchronize()
+        for (h, _), exp in zip(bufs, expected):
+            got = h.cpu().numpy()
+            assert np.all(got[:, 3] == 1.0)
+            assert np.array_equal(got.view(np.uint32), exp.view(np.uint32))
+    b.close()
