@@ -289,7 +289,9 @@ typedef struct kt_tune_entry {
 kt_status kt_context_autotune(kt_context* ctx, void* stream, const kt_camera* cam, uint32_t reps,
                               const kt_tuning* candidates, uint32_t n_candidates, kt_tune_entry* table,
                               uint32_t* n_entries);
-/* bloom_horizontal (cuda/kernel.cu:144-173): dev float4 hdr -> dev float4 bloom. */
+/* The post entry points read and write float4 pixels: hdr and bloom must be 16-byte aligned
+ * (KT_ERR_INVALID_ARG otherwise), image_out 4-byte aligned.
+ * bloom_horizontal (cuda/kernel.cu:144-173): dev float4 hdr -> dev float4 bloom. */
 kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom);
 /* post_process (cuda/kernel.cu:175-251): vertical blur + composite + ACES + sRGB + pack to
  * 0x00RRGGBB.  bloom may be NULL when bloom is inactive. */

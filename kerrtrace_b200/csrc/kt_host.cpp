@@ -908,8 +908,11 @@ kt_status kt_fma_peak(int device, uint32_t iters, double* tflops, float* ms) {
     return KT_OK;
 }
 
+static bool misaligned(const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) != 0; }
+
 kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, float* bloom) {
     if (!ctx || !hdr || !bloom) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (misaligned(hdr, 16) || misaligned(bloom, 16)) return fail(KT_ERR_INVALID_ARG, "hdr and bloom must be 16-byte aligned");
     DeviceGuard g(ctx->device);
     const cudaError_t e = ktd::launch_bloom_horizontal(ctx->post, reinterpret_cast<const float4*>(hdr),
                                                        reinterpret_cast<float4*>(bloom), (cudaStream_t)stream);
@@ -919,6 +922,8 @@ kt_status kt_bloom_horizontal(kt_context* ctx, void* stream, const float* hdr, f
 
 kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const float* bloom, uint32_t* image_out) {
     if (!ctx || !hdr || !image_out || (ctx->post.active && !bloom)) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (misaligned(hdr, 16) || misaligned(bloom, 16) || misaligned(image_out, 4))
+        return fail(KT_ERR_INVALID_ARG, "hdr and bloom must be 16-byte aligned, image_out 4-byte aligned");
     DeviceGuard g(ctx->device);
     const cudaError_t e = ktd::launch_post_process(ctx->post, reinterpret_cast<const float4*>(hdr),
                                                    reinterpret_cast<const float4*>(bloom), image_out,
@@ -929,6 +934,8 @@ kt_status kt_post_process(kt_context* ctx, void* stream, const float* hdr, const
 
 kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_t* image_out) {
     if (!ctx || !hdr || !image_out) return fail(KT_ERR_INVALID_ARG, "NULL argument");
+    if (misaligned(hdr, 16) || misaligned(image_out, 4))
+        return fail(KT_ERR_INVALID_ARG, "hdr must be 16-byte aligned, image_out 4-byte aligned");
     DeviceGuard g(ctx->device);
     const cudaError_t e = ktd::launch_post_fused(ctx->post, reinterpret_cast<const float4*>(hdr), image_out,
                                                  ctx->bloom_scratch, (cudaStream_t)stream);

@@ -31,7 +31,8 @@ def _hdr_input(torch, cfg, seed):
 
 @pytest.mark.parametrize("name,size,radius", [("t1", None, None), ("t2", None, None), ("c2", (333, 190), None),
                                               ("c2", (64, 40), 48.0), ("t1", (50, 70), 0.0),
-                                              ("c2", (96, 300), 70.0)])
+                                              ("c2", (96, 300), 70.0), ("c2", (72, 260), 95.0),
+                                              ("c2", (80, 90), 100.0), ("t1", (1, 1), None)])
 def test_post_bit_identical_to_reference(cuda, orc, name, size, radius):
     cfg, _ = workloads.scene(name)
     if size:
@@ -69,3 +70,26 @@ def test_post_bit_identical_to_reference(cuda, orc, name, size, radius):
     assert d.max() <= 1, np.bincount(d)
     ctx.close()
     ref.close()
+
+
+def test_post_rejects_misaligned_buffers(cuda):
+    """The post entry points read and write float4 pixels: a pointer off the 16-byte grid (or an
+    image pointer off the 4-byte grid) is refused on the host, before any launch."""
+    cfg, _ = workloads.scene("t1")
+    n = cfg.width * cfg.height
+    ctx = kt.Context(cfg)
+    hdr = cuda.zeros((n + 1, 4), device="cuda")
+    bloom = cuda.zeros((n + 1, 4), device="cuda")
+    img = cuda.zeros(n + 1, dtype=cuda.int32, device="cuda")
+    calls = [lambda: ctx.post_fused(hdr.data_ptr() + 4, img.data_ptr()),
+             lambda: ctx.post_fused(hdr.data_ptr(), img.data_ptr() + 2),
+             lambda: ctx.bloom_horizontal(hdr.data_ptr() + 8, bloom.data_ptr()),
+             lambda: ctx.bloom_horizontal(hdr.data_ptr(), bloom.data_ptr() + 4),
+             lambda: ctx.post_process(hdr.data_ptr(), bloom.data_ptr() + 12, img.data_ptr())]
+    for call in calls:
+        with pytest.raises(kt.KtError) as e:
+            call()
+        assert e.value.status == kt.KT_ERR_INVALID_ARG and "aligned" in str(e.value)
+    ctx.post_fused(hdr.data_ptr(), img.data_ptr())  # aligned: runs
+    cuda.cuda.synchronize()
+    ctx.close()
