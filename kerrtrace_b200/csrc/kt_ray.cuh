@@ -146,11 +146,13 @@ __device__ __forceinline__ bool ray_start(RayRun<R>& ry, const Camera& cam, cons
 
 // Tolerance of the step starting at s (cuda/kerr_trace.cuh:67-73): scaled by the Kerr-Schild
 // potential from 5x far away down to 0 at Hk >= 0.3 (reference), or down to 1x (stated physics).
+// rc is the Kerr-Schild radius of s; the step that ends at s has computed it already for its
+// horizon and escape tests (the same ks_radius of the same state), so ray_advance passes that
+// value on instead of evaluating it again at the next step's start.
 template <class R, int MODE>
-__device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
+__device__ __forceinline__ R step_tolerance_at(R rc, const R* s, const Scene& sc) {
     using O = Ops<R>;
     const R aa = sc_aa<R>(sc), M = sc_M<R>(sc);
-    const R rc = ks_radius<R>(s[0], s[1], s[2], aa);
     const R rc2 = rc * rc;
     const R denH = O::fma(rc2, rc2, aa * s[1] * s[1]);
     const R Hk = M * rc * rc2 * O::fdiv(R(1), denH);
@@ -159,6 +161,10 @@ __device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
     const R base = sc_tol<R>(sc);
     if (MODE != 1) return base * (R(5) - R(5) * t);
     return base * (R(5) - R(4) * t);
+}
+template <class R, int MODE>
+__device__ __forceinline__ R step_tolerance(const R* s, const Scene& sc) {
+    return step_tolerance_at<R, MODE>(ks_radius<R>(s[0], s[1], s[2], sc_aa<R>(sc)), s, sc);
 }
 
 // Blackbody colour for the FP64 path: software interpolation of the LUT in double.
@@ -329,7 +335,8 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
     using O = Ops<R>;
     using C = DP<R>;
     const R a = sc_a<R>(sc), aa = sc_aa<R>(sc), M = sc_M<R>(sc);
-    if (ry.attempt == 0) ry.tol = step_tolerance<R, MODE>(ry.s, sc);
+    // the first step's tolerance; later steps get theirs from the commit of the step before
+    if (ry.attempt == 0 && ry.step == 0) ry.tol = step_tolerance<R, MODE>(ry.s, sc);
     if (!ry.have_k1) {
         hamilton_rhs<R, EXACT>(ry.s, ry.pt, a, aa, M, ry.k1);
         ry.have_k1 = true;
@@ -417,7 +424,9 @@ __device__ __forceinline__ bool ray_advance(RayRun<R>& ry, const Scene& sc, uint
         return true;
     }
     ry.step++;
-    return !(ry.step < sc.max_steps && tau_alive<R>(ry.tau, sc));
+    const bool done = !(ry.step < sc.max_steps && tau_alive<R>(ry.tau, sc));
+    if (!done) ry.tol = step_tolerance_at<R, MODE>(r_now, ry.s, sc);
+    return done;
 }
 
 // =========================================================================================
@@ -563,9 +572,10 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
     using CD = DP<double>;
     const float a = sc.a, aa = sc.aa, M = sc.M;
     const float pt = (float)ry.pt;
-    if (ry.attempt == 0) {
-        ry.tol = step_tolerance<float, 1>(ry.s, sc);
-        ry.zone = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa) < sc.zone_r;
+    if (ry.attempt == 0 && ry.step == 0) {  // later steps: set by the commit of the step before
+        const float rc = ks_radius<float>(ry.s[0], ry.s[1], ry.s[2], aa);
+        ry.tol = step_tolerance_at<float, 1>(rc, ry.s, sc);
+        ry.zone = rc < sc.zone_r;
     }
     if (!ry.have_k1) {
         hamilton_rhs<float, EXACT>(ry.s, pt, a, aa, M, ry.k1);
@@ -736,7 +746,12 @@ __device__ __forceinline__ bool ray_advance_mixed(RayRun<Mixed>& ry, const Scene
         return true;
     }
     ry.step++;
-    return !(ry.step < sc.max_steps && ry.tau > sc.cutoff_gt);
+    const bool done = !(ry.step < sc.max_steps && ry.tau > sc.cutoff_gt);
+    if (!done) {
+        ry.tol = step_tolerance_at<float, 1>(r_now, ry.s, sc);
+        ry.zone = r_now < sc.zone_r;
+    }
+    return done;
 }
 
 // Uniform entry points used by the kernels for every arithmetic type.
