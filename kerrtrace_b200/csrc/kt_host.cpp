@@ -955,18 +955,23 @@ struct kt_frame {
     uint32_t* host_image = nullptr;  // pinned
     uint32_t* err = nullptr;
     uint32_t* host_err = nullptr;    // pinned, 2 words
-    cudaEvent_t computed = nullptr;  // trace + post done (on the render stream)
+    cudaEvent_t traced = nullptr;    // trace done (on the render stream)
+    cudaEvent_t computed = nullptr;  // post done (on the post stream)
     cudaEvent_t ready = nullptr;     // image and error word in pinned memory (on the copy stream)
     bool has_event = false;
     bool used = false;               // `ready` has been recorded at least once
 };
 
-// Frames render on the legacy default stream (cudarc's default_stream(), like the reference) and
-// come back to pinned memory on a non-blocking copy stream, so that with two frames in flight
-// the copy of one overlaps the trace of the next.
+// Frames are traced on the legacy default stream (cudarc's default_stream(), like the reference),
+// post-processed on a non-blocking stream of the highest priority and come back to pinned memory
+// on a non-blocking copy stream.  With two frames in flight the post passes of one frame run
+// while the next frame is traced: their blocks are dispatched ahead of the trace's remaining
+// blocks as SMs free up, and being latency-bound they fill issue slots that the FMA-bound trace
+// leaves.  The copy of one frame overlaps the trace of the next as well.
 struct kt_renderer {
     kt_context* ctx = nullptr;
     cudaStream_t stream = nullptr;   // the legacy default stream, like cudarc's default_stream()
+    cudaStream_t post = nullptr;     // non-blocking, highest priority: bloom and tone map
     cudaStream_t copy = nullptr;     // non-blocking device-to-host stream
     kt_frame frames[2];
     std::deque<uint32_t> pending;
@@ -989,8 +994,10 @@ void destroy_renderer(kt_renderer* r) {
             cudaFreeHost(f.host_err);
             if (f.ready) cudaEventDestroy(f.ready);
             if (f.computed) cudaEventDestroy(f.computed);
+            if (f.traced) cudaEventDestroy(f.traced);
         }
         if (r->copy) cudaStreamDestroy(r->copy);
+        if (r->post) cudaStreamDestroy(r->post);
         destroy_ctx(r->ctx);
     }
     delete r;
@@ -1012,9 +1019,12 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
     DeviceGuard g(device);
     const size_t px = (size_t)cfg->width * cfg->height;
     {
-        const cudaError_t e = cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking);
+        int least = 0, greatest = 0;
+        cudaError_t e = cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&r->post, cudaStreamNonBlocking, greatest);
         if (e != cudaSuccess) {
-            st = cuda_fail(e, "create copy stream");
+            st = cuda_fail(e, "create copy and post streams");
             destroy_renderer(r);
             return st;
         }
@@ -1029,6 +1039,7 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
             (e = cudaMallocHost(&f.host_err, 2 * sizeof(uint32_t))) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&f.ready, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&f.computed, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&f.traced, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaMemset(f.hdr, 0, px * 4 * sizeof(float))) != cudaSuccess ||
             (e = cudaMemset(f.bloom, 0, px * 4 * sizeof(float))) != cudaSuccess ||
             (e = cudaMemset(f.image, 0, px * sizeof(uint32_t))) != cudaSuccess ||
@@ -1092,9 +1103,12 @@ kt_status kt_renderer_submit_render(kt_renderer* r, const float cam_pos[3], cons
     KT_CUDA(cudaMemsetAsync(f.err, 0, 2 * sizeof(uint32_t), r->stream), "clear LUT error flag");
     kt_status st = kt_trace(r->ctx, r->stream, &cam, r->schedule, f.hdr, f.err);
     if (st != KT_OK) return st;
-    st = kt_post_fused(r->ctx, r->stream, f.hdr, f.image);
+    KT_CUDA(cudaEventRecord(f.traced, r->stream), "record trace event");
+    // post passes on their own stream (one at a time: they share the context's bloom buffer)
+    KT_CUDA(cudaStreamWaitEvent(r->post, f.traced, 0), "order the post passes after the trace");
+    st = kt_post_fused(r->ctx, r->post, f.hdr, f.image);
     if (st != KT_OK) return st;
-    KT_CUDA(cudaEventRecord(f.computed, r->stream), "record render event");
+    KT_CUDA(cudaEventRecord(f.computed, r->post), "record render event");
     KT_CUDA(cudaStreamWaitEvent(r->copy, f.computed, 0), "order the copy after the render");
     KT_CUDA(cudaMemcpyAsync(f.host_err, f.err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->copy), "read LUT error flag");
     KT_CUDA(cudaMemcpyAsync(f.host_image, f.image, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->copy), "copy image back");
