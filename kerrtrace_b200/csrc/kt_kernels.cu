@@ -689,11 +689,20 @@ __device__ __forceinline__ void load_weights(float* w, int R, float sigma, int t
     for (int i = tid; i <= 2 * R + 1; i += nthreads) w[i] = i <= 2 * R ? tap_weight(i - R, sigma) : 0.0f;
 }
 
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only); the bytes past src_bytes are
+// zero-filled and nothing is read when src_bytes is 0.  Both addresses are 16-byte aligned.
+__device__ __forceinline__ void copy16_async(float4* dst, const float4* src, int src_bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Horizontal pass (bloom_horizontal, cuda/kernel.cu:144-173): a block makes a 32-row x 64-column
 // tile.  Lane = row, warp = a kBJ-column chunk, so every tap test is uniform across the warp.
-// The 32 source rows (64 + 2R columns) are staged with coalesced loads at an odd float4 row
-// stride (conflict-free column reads); the results go back through the same shared memory for
-// coalesced stores.
+// The 32 source rows (64 + 2R columns) are staged at an odd float4 row stride (conflict-free
+// column reads): warp w copies rows w, w + 8, w + 16 and w + 24, its lanes taking consecutive
+// float4 of a row (coalesced, no index division), every copy in flight before the first is
+// waited for.  The results go back through the same shared memory for coalesced stores.
 constexpr int kHRows = 32, kHWarps = 8, kHCols = kHWarps * kBJ;
 
 __host__ __device__ constexpr int bloom_h_stride(int R) { return (kHCols + 2 * R) | 1; }
@@ -710,23 +719,30 @@ __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostPar
     const int x0 = blockIdx.x * kHCols, y0 = blockIdx.y * kHRows;
     const int tid = threadIdx.x;
     load_weights(w, R, pp.sigma, tid, blockDim.x);
-    const int total = kHRows * segw;
-    for (int j0 = tid; j0 < total; j0 += 4 * (int)blockDim.x) {  // 4 loads in flight per thread
-        float4 v[4];
-        int at[4];
+    {
+        const int wr = tid >> 5, ln = tid & 31;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int j = j0 + b * (int)blockDim.x;
-            const int r = j / segw, c = j - r * segw;
-            const int gy = y0 + r, gx = x0 - R + c;
-            at[b] = j < total ? r * stride + c : -1;
-            v[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (j < total && gy < pp.height && gx >= 0 && gx < pp.width)
-                v[b] = bloom_source(__ldg(hdr + (size_t)gy * pp.width + gx), pp);
+        for (int q = 0; q < kHRows / kHWarps; ++q) {
+            const int r = wr + q * kHWarps, gy = y0 + r;
+            const bool row_in = gy < pp.height;
+            const float4* src_row = hdr + (size_t)(row_in ? gy : 0) * pp.width;
+            for (int c = ln; c < segw; c += 32) {
+                const int gx = x0 - R + c;
+                const bool in = row_in && gx >= 0 && gx < pp.width;
+                copy16_async(stage + r * stride + c, src_row + (in ? gx : 0), in ? 16 : 0);
+            }
         }
+        copy_async_wait_all();
+        if (pp.mode == 1) {  // stated physics: the bloom source of each in-image value, in place
 #pragma unroll
-        for (int b = 0; b < 4; ++b)
-            if (at[b] >= 0) stage[at[b]] = v[b];
+            for (int q = 0; q < kHRows / kHWarps; ++q) {
+                const int r = wr + q * kHWarps, gy = y0 + r;
+                for (int c = ln; c < segw; c += 32) {
+                    const int gx = x0 - R + c;
+                    if (gy < pp.height && gx >= 0 && gx < pp.width) stage[r * stride + c] = bloom_source(stage[r * stride + c], pp);
+                }
+            }
+        }
     }
     __syncthreads();
     if (tid < kHCols) wsum[tid] = weight_sum(x0 + tid, pp.width, w, R);
