@@ -14,8 +14,10 @@
 //   bloom_h_kernel          horizontal normalised Gaussian, register-blocked over staged rows
 //   post_v_kernel           vertical Gaussian streamed from the bloom buffer + composite, ACES,
 //                           sRGB OETF, 0x00RRGGBB pack
+//   post_vt_kernel          the same over the column-major bloom buffer of the fused post
 //   tonemap_kernel          tone map alone (bloom inactive)
-// kt_post_fused runs both passes over a bloom buffer that the context owns.  The post kernels
+// kt_post_fused runs both passes over a bloom buffer that the context owns, stored column-major
+// between them: bloom_h_kernel<true> writes it, post_vt_kernel stages its columns like rows.  The post kernels
 // produce the reference's bits: same tap order, weights, division and tone-map expressions.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -707,6 +709,31 @@ constexpr int kHRows = 32, kHWarps = 8, kHCols = kHWarps * kBJ;
 
 __host__ __device__ constexpr int bloom_h_stride(int R) { return (kHCols + 2 * R) | 1; }
 
+// Stages kHRows lines of a line-major source (line l at src + l * pitch; n_lines lines of
+// n_pos values) into `stage`: lines line0 .. line0 + kHRows - 1, positions p0 - R ..
+// p0 + kHCols + R - 1, zero outside the source.  Returns after the block's copies have landed
+// (a barrier follows).
+__device__ __forceinline__ void stage_lines(float4* stage, int stride, int segw, const float4* __restrict__ src,
+                                            size_t pitch, int n_lines, int n_pos, int line0, int p0, int R,
+                                            int tid) {
+    const int wr = tid >> 5, ln = tid & 31;
+#pragma unroll
+    for (int q = 0; q < kHRows / kHWarps; ++q) {
+        const int r = wr + q * kHWarps, gl = line0 + r;
+        const bool line_in = gl < n_lines;
+        const float4* src_line = src + (line_in ? (size_t)gl * pitch : 0);
+        for (int c = ln; c < segw; c += 32) {
+            const int gp = p0 - R + c;
+            const bool in = line_in && gp >= 0 && gp < n_pos;
+            copy16_async(stage + r * stride + c, src_line + (in ? gp : 0), in ? 16 : 0);
+        }
+    }
+    copy_async_wait_all();
+}
+
+// TRANSPOSED writes the bloom buffer column-major (bloom[x * height + y]): the layout that the
+// fused post's vertical pass (post_vt_kernel) stages like this pass stages its rows.
+template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostParams pp,
                                                                     const float4* __restrict__ hdr,
                                                                     float4* __restrict__ bloom) {
@@ -719,28 +746,15 @@ __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostPar
     const int x0 = blockIdx.x * kHCols, y0 = blockIdx.y * kHRows;
     const int tid = threadIdx.x;
     load_weights(w, R, pp.sigma, tid, blockDim.x);
-    {
+    stage_lines(stage, stride, segw, hdr, (size_t)pp.width, pp.height, pp.width, y0, x0, R, tid);
+    if (pp.mode == 1) {  // stated physics: the bloom source of each in-image value, in place
         const int wr = tid >> 5, ln = tid & 31;
 #pragma unroll
         for (int q = 0; q < kHRows / kHWarps; ++q) {
             const int r = wr + q * kHWarps, gy = y0 + r;
-            const bool row_in = gy < pp.height;
-            const float4* src_row = hdr + (size_t)(row_in ? gy : 0) * pp.width;
             for (int c = ln; c < segw; c += 32) {
                 const int gx = x0 - R + c;
-                const bool in = row_in && gx >= 0 && gx < pp.width;
-                copy16_async(stage + r * stride + c, src_row + (in ? gx : 0), in ? 16 : 0);
-            }
-        }
-        copy_async_wait_all();
-        if (pp.mode == 1) {  // stated physics: the bloom source of each in-image value, in place
-#pragma unroll
-            for (int q = 0; q < kHRows / kHWarps; ++q) {
-                const int r = wr + q * kHWarps, gy = y0 + r;
-                for (int c = ln; c < segw; c += 32) {
-                    const int gx = x0 - R + c;
-                    if (gy < pp.height && gx >= 0 && gx < pp.width) stage[r * stride + c] = bloom_source(stage[r * stride + c], pp);
-                }
+                if (gy < pp.height && gx >= 0 && gx < pp.width) stage[r * stride + c] = bloom_source(stage[r * stride + c], pp);
             }
         }
     }
@@ -769,10 +783,18 @@ __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostPar
         stage[lane * ostride + cb + j] = make_float4(ax, ay, az, 0.0f);
     }
     __syncthreads();
-    for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
-        const int r = j / kHCols, c = j - r * kHCols;
-        const int gy = y0 + r, gx = x0 + c;
-        if (gy < pp.height && gx < pp.width) bloom[(size_t)gy * pp.width + gx] = stage[r * ostride + c];
+    if (TRANSPOSED) {  // lanes on consecutive rows of one column: coalesced column-major stores
+        for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
+            const int c = j / kHRows, r = j - c * kHRows;
+            const int gy = y0 + r, gx = x0 + c;
+            if (gy < pp.height && gx < pp.width) bloom[(size_t)gx * pp.height + gy] = stage[r * ostride + c];
+        }
+    } else {
+        for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
+            const int r = j / kHCols, c = j - r * kHCols;
+            const int gy = y0 + r, gx = x0 + c;
+            if (gy < pp.height && gx < pp.width) bloom[(size_t)gy * pp.width + gx] = stage[r * ostride + c];
+        }
     }
 }
 
@@ -835,6 +857,60 @@ __global__ void __launch_bounds__(kVThreads) post_v_kernel(const PostParams pp,
     }
 }
 
+// Vertical pass of the fused post over the column-major bloom buffer that bloom_h_kernel<true>
+// writes: a block makes a 32-column x 64-row tile.  Lane = column, warp = a kBJ-row chunk; the
+// block stages its 32 columns (64 + 2R rows each) exactly as the horizontal pass stages rows,
+// so every source value is read from L2 once per tile instead of once per kBJ outputs, then
+// blurs, composites, tone-maps and packs with the arithmetic of post_v_kernel (same bits).
+__global__ void __launch_bounds__(kHRows * kHWarps) post_vt_kernel(const PostParams pp,
+                                                                    const float4* __restrict__ hdr,
+                                                                    const float4* __restrict__ bloom_t,
+                                                                    uint32_t* __restrict__ image) {
+    extern __shared__ float4 smem4[];
+    const int R = pp.radius;
+    const int segw = kHCols + 2 * R, stride = bloom_h_stride(R);
+    float4* stage = smem4;                                             // kHRows x stride
+    float* w = reinterpret_cast<float*>(stage + kHRows * stride);      // 2R + 2
+    float* wsum = w + 2 * R + 2;                                       // kHCols
+    const int x0 = blockIdx.x * kHRows, y0 = blockIdx.y * kHCols;
+    const int tid = threadIdx.x;
+    load_weights(w, R, pp.sigma, tid, blockDim.x);
+    stage_lines(stage, stride, segw, bloom_t, (size_t)pp.height, pp.width, pp.height, x0, y0, R, tid);
+    __syncthreads();
+    if (tid < kHCols) wsum[tid] = weight_sum(y0 + tid, pp.height, w, R);
+    const int lane = tid & 31, cb = (tid >> 5) * kBJ;
+    const float4* col = stage + lane * stride + cb;
+    auto load = [col](int k) { return col[k]; };
+    float acc[kBJ][3];
+    const int ys = y0 + cb;
+    if (2 * R >= kBJ - 1 && ys - R >= 0 && ys + kBJ - 1 + R < pp.height)
+        blur_interior(load, w, R, acc);
+    else
+        blur_edge(load, w, R, ys, pp.height, acc);
+    __syncthreads();  // wsum written
+    const int x = x0 + lane;
+    if (x >= pp.width) return;
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j) {
+        const int y = ys + j;
+        if (y >= pp.height) break;
+        const size_t idx = (size_t)y * pp.width + x;
+        const float4 base = __ldg(hdr + idx);
+        float fr = base.x, fg = base.y, fb = base.z;
+        const float ws = wsum[cb + j];
+        float ax = acc[j][0], ay = acc[j][1], az = acc[j][2];
+        if (ws > 0.0f) {
+            ax /= ws;
+            ay /= ws;
+            az /= ws;
+        }
+        fr += ax * pp.intensity;
+        fg += ay * pp.intensity;
+        fb += az * pp.intensity;
+        image[idx] = tone_pack(fr, fg, fb);
+    }
+}
+
 // Tone map only (bloom inactive): one thread per pixel.
 __global__ void tonemap_kernel(const PostParams pp, const float4* __restrict__ hdr,
                                uint32_t* __restrict__ image) {
@@ -861,10 +937,10 @@ cudaError_t launch_bloom_horizontal(const PostParams& pp, const float4* hdr, flo
     if (pp.width <= 0 || pp.height <= 0) return cudaSuccess;
     const size_t sm = bloom_h_smem(pp.radius);
     if (sm > kSmemLimit) return cudaErrorInvalidValue;
-    cudaError_t e = set_smem((const void*)bloom_h_kernel, sm);
+    cudaError_t e = set_smem((const void*)bloom_h_kernel<false>, sm);
     if (e != cudaSuccess) return e;
     const dim3 grid((pp.width + kHCols - 1) / kHCols, (pp.height + kHRows - 1) / kHRows);
-    bloom_h_kernel<<<grid, kHRows * kHWarps, sm, st>>>(pp, hdr, bloom);
+    bloom_h_kernel<false><<<grid, kHRows * kHWarps, sm, st>>>(pp, hdr, bloom);
     return cudaGetLastError();
 }
 
@@ -914,9 +990,17 @@ cudaError_t launch_post_fused(const PostParams& pp, const float4* hdr, uint32_t*
         return cudaGetLastError();
     }
     if (!scratch) return cudaErrorInvalidValue;
-    const cudaError_t e = launch_bloom_horizontal(pp, hdr, scratch, st);
+    // both passes through the context's scratch, column-major in between (never seen by callers)
+    const size_t sm = bloom_h_smem(pp.radius);
+    if (sm > kSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e = set_smem((const void*)bloom_h_kernel<true>, sm);
+    if (e == cudaSuccess) e = set_smem((const void*)post_vt_kernel, sm);
     if (e != cudaSuccess) return e;
-    return launch_post_process(pp, hdr, scratch, image, st);
+    const dim3 gh((pp.width + kHCols - 1) / kHCols, (pp.height + kHRows - 1) / kHRows);
+    bloom_h_kernel<true><<<gh, kHRows * kHWarps, sm, st>>>(pp, hdr, scratch);
+    const dim3 gv((pp.width + kHRows - 1) / kHRows, (pp.height + kHCols - 1) / kHCols);
+    post_vt_kernel<<<gv, kHRows * kHWarps, sm, st>>>(pp, hdr, scratch, image);
+    return cudaGetLastError();
 }
 
 }  // namespace ktd
