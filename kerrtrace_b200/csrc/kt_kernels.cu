@@ -702,7 +702,7 @@ __device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.w
 // Horizontal pass (bloom_horizontal, cuda/kernel.cu:144-173): a block makes a 32-row x 64-column
 // tile.  Lane = row, warp = a kBJ-column chunk, so every tap test is uniform across the warp.
 // The 32 source rows (64 + 2R columns) are staged at an odd float4 row stride (conflict-free
-// column reads): warp w copies rows w, w + 8, w + 16 and w + 24, its lanes taking consecutive
+// column reads): warp w copies rows w, w + kHWarps, ..., its lanes taking consecutive
 // float4 of a row (coalesced, no index division), every copy in flight before the first is
 // waited for.  The results go back through the same shared memory for coalesced stores.
 constexpr int kHRows = 32, kHWarps = 8, kHCols = kHWarps * kBJ;
@@ -717,9 +717,8 @@ __device__ __forceinline__ void stage_lines(float4* stage, int stride, int segw,
                                             size_t pitch, int n_lines, int n_pos, int line0, int p0, int R,
                                             int tid) {
     const int wr = tid >> 5, ln = tid & 31;
-#pragma unroll
-    for (int q = 0; q < kHRows / kHWarps; ++q) {
-        const int r = wr + q * kHWarps, gl = line0 + r;
+    for (int r = wr; r < kHRows; r += kHWarps) {
+        const int gl = line0 + r;
         const bool line_in = gl < n_lines;
         const float4* src_line = src + (line_in ? (size_t)gl * pitch : 0);
         for (int c = ln; c < segw; c += 32) {
@@ -749,9 +748,8 @@ __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostPar
     stage_lines(stage, stride, segw, hdr, (size_t)pp.width, pp.height, pp.width, y0, x0, R, tid);
     if (pp.mode == 1) {  // stated physics: the bloom source of each in-image value, in place
         const int wr = tid >> 5, ln = tid & 31;
-#pragma unroll
-        for (int q = 0; q < kHRows / kHWarps; ++q) {
-            const int r = wr + q * kHWarps, gy = y0 + r;
+        for (int r = wr; r < kHRows; r += kHWarps) {
+            const int gy = y0 + r;
             for (int c = ln; c < segw; c += 32) {
                 const int gx = x0 - R + c;
                 if (gy < pp.height && gx >= 0 && gx < pp.width) stage[r * stride + c] = bloom_source(stage[r * stride + c], pp);
