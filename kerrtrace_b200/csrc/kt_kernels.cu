@@ -704,7 +704,7 @@ __device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.w
 // The 32 source rows (64 + 2R columns) are staged at an odd float4 row stride (conflict-free
 // column reads): warp w copies rows w, w + kHWarps, ..., its lanes taking consecutive
 // float4 of a row (coalesced, no index division), every copy in flight before the first is
-// waited for.  The results go back through the same shared memory for coalesced stores.
+// waited for.
 constexpr int kHRows = 32, kHWarps = 8, kHCols = kHWarps * kBJ;
 
 __host__ __device__ constexpr int bloom_h_stride(int R) { return (kHCols + 2 * R) | 1; }
@@ -731,7 +731,9 @@ __device__ __forceinline__ void stage_lines(float4* stage, int stride, int segw,
 }
 
 // TRANSPOSED writes the bloom buffer column-major (bloom[x * height + y]): the layout that the
-// fused post's vertical pass (post_vt_kernel) stages like this pass stages its rows.
+// fused post's vertical pass (post_vt_kernel) stages like this pass stages its rows.  Lanes
+// being rows, it stores straight from registers; the row-major output goes back through shared
+// memory for coalesced stores.
 template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostParams pp,
                                                                     const float4* __restrict__ hdr,
@@ -768,6 +770,24 @@ __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostPar
     else
         blur_edge(load, w, R, xs, pp.width, acc);
     __syncthreads();  // staged sources no longer read; wsum written
+    if (TRANSPOSED) {  // lane = row: each output column's 32 rows are one coalesced store
+        const int gy = y0 + lane;
+        if (gy >= pp.height) return;
+#pragma unroll
+        for (int j = 0; j < kBJ; ++j) {
+            const int gx = xs + j;
+            if (gx >= pp.width) break;
+            const float ws = wsum[cb + j];
+            float ax = acc[j][0], ay = acc[j][1], az = acc[j][2];
+            if (ws > 0.0f) {
+                ax /= ws;
+                ay /= ws;
+                az /= ws;
+            }
+            bloom[(size_t)gx * pp.height + gy] = make_float4(ax, ay, az, 0.0f);
+        }
+        return;
+    }
     constexpr int ostride = kHCols + 1;
 #pragma unroll
     for (int j = 0; j < kBJ; ++j) {
@@ -781,18 +801,10 @@ __global__ void __launch_bounds__(kHRows * kHWarps) bloom_h_kernel(const PostPar
         stage[lane * ostride + cb + j] = make_float4(ax, ay, az, 0.0f);
     }
     __syncthreads();
-    if (TRANSPOSED) {  // lanes on consecutive rows of one column: coalesced column-major stores
-        for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
-            const int c = j / kHRows, r = j - c * kHRows;
-            const int gy = y0 + r, gx = x0 + c;
-            if (gy < pp.height && gx < pp.width) bloom[(size_t)gx * pp.height + gy] = stage[r * ostride + c];
-        }
-    } else {
-        for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
-            const int r = j / kHCols, c = j - r * kHCols;
-            const int gy = y0 + r, gx = x0 + c;
-            if (gy < pp.height && gx < pp.width) bloom[(size_t)gy * pp.width + gx] = stage[r * ostride + c];
-        }
+    for (int j = tid; j < kHRows * kHCols; j += blockDim.x) {
+        const int r = j / kHCols, c = j - r * kHCols;
+        const int gy = y0 + r, gx = x0 + c;
+        if (gy < pp.height && gx < pp.width) bloom[(size_t)gy * pp.width + gx] = stage[r * ostride + c];
     }
 }
 
@@ -888,13 +900,16 @@ __global__ void __launch_bounds__(kHRows * kHWarps) post_vt_kernel(const PostPar
     __syncthreads();  // wsum written
     const int x = x0 + lane;
     if (x >= pp.width) return;
+    float4 base[kBJ];  // all of a thread's composite sources in flight before the first is used
+#pragma unroll
+    for (int j = 0; j < kBJ; ++j)
+        base[j] = ys + j < pp.height ? __ldg(hdr + (size_t)(ys + j) * pp.width + x) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int j = 0; j < kBJ; ++j) {
         const int y = ys + j;
         if (y >= pp.height) break;
         const size_t idx = (size_t)y * pp.width + x;
-        const float4 base = __ldg(hdr + idx);
-        float fr = base.x, fg = base.y, fb = base.z;
+        float fr = base[j].x, fg = base[j].y, fb = base[j].z;
         const float ws = wsum[cb + j];
         float ax = acc[j][0], ay = acc[j][1], az = acc[j][2];
         if (ws > 0.0f) {
