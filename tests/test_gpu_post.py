@@ -93,3 +93,46 @@ def test_post_rejects_misaligned_buffers(cuda):
     ctx.post_fused(hdr.data_ptr(), img.data_ptr())  # aligned: runs
     cuda.cuda.synchronize()
     ctx.close()
+
+
+@pytest.mark.parametrize("size,radius", [(None, None), ((333, 190), 24.0), ((64, 40), 48.0), ((1, 1), None)])
+def test_stated_physics_bloom_threshold(cuda, orc, size, radius):
+    """Stated physics blooms only the luminance above the threshold (the source of each in-image
+    value is scaled in place after staging).  The fused pair (column-major bloom buffer) equals
+    the separate passes bit for bit, and both agree with the oracle's double-precision post to
+    one code value per channel."""
+    cfg, _ = workloads.scene("c2")
+    cfg = workloads.scaled(cfg, *(size or (160, 96)))
+    cfg.mode = 1
+    cfg.bloom_threshold = 1.0
+    if radius is not None:
+        cfg.bloom_radius = radius
+    R, sigma, active = _bloom_consts(cfg)
+    assert active
+    hdr = _hdr_input(cuda, cfg, 11)
+    n = cfg.width * cfg.height
+    ctx = kt.Context(cfg)
+    bloom = cuda.zeros((n, 4), device="cuda")
+    img_s = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    img_f = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    ctx.bloom_horizontal(hdr.data_ptr(), bloom.data_ptr())
+    ctx.post_process(hdr.data_ptr(), bloom.data_ptr(), img_s.data_ptr())
+    ctx.post_fused(hdr.data_ptr(), img_f.data_ptr())
+    cuda.cuda.synchronize()
+    i_s, i_f = (t.cpu().numpy().view(np.uint32) for t in (img_s, img_f))
+    assert np.array_equal(i_s, i_f)
+    exp = orc.post(hdr.cpu().numpy(), cfg.width, cfg.height, R, sigma, cfg.bloom_intensity, 1, cfg.bloom_threshold)
+    d = np.max(np.abs(np.stack([(i_f >> s) & 255 for s in (16, 8, 0)]).astype(int) -
+                      np.stack([(exp >> s) & 255 for s in (16, 8, 0)]).astype(int)), axis=0)
+    assert d.max() <= 1, np.bincount(d)
+    # the threshold matters: the reference semantics' bloom of the same input differs
+    cfg0 = cfg.copy()
+    cfg0.mode = 0
+    ctx0 = kt.Context(cfg0)
+    img_0 = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    ctx0.post_fused(hdr.data_ptr(), img_0.data_ptr())
+    cuda.cuda.synchronize()
+    if n > 1:
+        assert not np.array_equal(img_0.cpu().numpy().view(np.uint32), i_f)
+    ctx0.close()
+    ctx.close()
