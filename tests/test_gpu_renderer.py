@@ -84,8 +84,9 @@ def test_both_schedules_render_the_same_frame(cuda):
 
 
 def test_pipelined_frames_keep_their_own_camera(cuda):
-    """Two frames in flight (the copy of one overlapping the trace of the next): each frame
-    handed back is the image of the camera it was submitted with."""
+    """Two frames in flight (the post passes and the copy of one overlapping the trace of the
+    next, on their own streams): each frame handed back is the image of the camera it was
+    submitted with."""
     cfg, _ = workloads.scene("t2")
     cams = [kt.orbit_camera(40.0, 50.0 + 6.0 * k, 30.0) for k in range(6)]
     ctx = kt.Context(cfg)
