@@ -731,6 +731,25 @@ def adjoint_leg(local, reps: int, size: int = 512) -> dict:
                          "FP32 records replayed in FP64 arithmetic", "masked_pixels": int(mask.sum()),
                          "adjoint": ga, "central_differences": ref,
                          "rel_err": [abs(ga[j] - ref[j]) / max(abs(ref[j]), 1e-300) for j in range(4)]}
+        if prec == kt.PREC_FP32:
+            # the FP64 adjoint of the same FP32 records (kt_diff_backward_fp64): the model the
+            # central differences above measure, differentiated in double
+            d.backward_fp64(wm.data_ptr(), g.data_ptr())
+            torch.cuda.synchronize()
+            g64 = g.cpu().tolist()
+            tb64 = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                d.backward_fp64(w.data_ptr(), g.data_ptr())
+                e1.record()
+                torch.cuda.synchronize()
+                tb64.append(e0.elapsed_time(e1))
+            b64 = sorted(tb64)[len(tb64) // 2]
+            r["backward_fp64_records"] = {
+                "backward_ms": round(b64, 3), "adjoint_mrays_s": round(n / (f_ms + b64) / 1e3, 2),
+                "cost_ratio": round((f_ms + b64) / f_ms, 2), "adjoint": g64,
+                "rel_err": [abs(g64[j] - ref[j]) / max(abs(ref[j]), 1e-300) for j in range(4)]}
         out[pname] = r
         d.close()
     return out

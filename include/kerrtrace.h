@@ -490,6 +490,14 @@ kt_status kt_diff_replay_fp64(kt_diff* d, void* stream, const kt_diff_params* th
                               uint32_t* flags_out, uint32_t* err_word, float* hdr_out);
 /* dl_dhdr: device float4 per pixel (w ignored); grad_out: device, 4 doubles (overwritten). */
 kt_status kt_diff_backward(kt_diff* d, void* stream, const float* dl_dhdr, double* grad_out);
+/* The adjoint of the model kt_diff_replay_fp64 evaluates: for an FP32 object, its FP32 records
+ * (step sizes, shaded crossings) replayed and differentiated in double from the double start of
+ * each ray, so that the float rounding of the recorded trajectory does not enter the gradient
+ * (the r_out derivative is the most sensitive to it); it costs about as much as the FP64 adjoint.
+ * For an FP64 object it is kt_diff_backward.  Arguments as kt_diff_backward; it uploads the
+ * double tables of the recorded theta into the buffers that kt_diff_replay_fp64 uses, so the two
+ * are ordered on one stream. */
+kt_status kt_diff_backward_fp64(kt_diff* d, void* stream, const float* dl_dhdr, double* grad_out);
 kt_status kt_diff_get_info(kt_diff* d, kt_diff_info* info);  /* synchronises with the device */
 /* The orbit camera of the diff trace and its derivative in the inclination (degrees). */
 kt_status kt_diff_orbit_camera(float observer_r, float inclination_deg, float azimuth_deg, float fov_deg,

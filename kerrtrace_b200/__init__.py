@@ -201,6 +201,7 @@ SIGNATURES = [
     ("kt_diff_replay", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtDiffParams), C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p]),
     ("kt_diff_backward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("kt_diff_backward_fp64", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("kt_diff_replay_fp64", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(KtDiffParams), C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]),
     ("kt_diff_get_info", C.c_int, [C.c_void_p, C.POINTER(KtDiffInfo)]),
@@ -476,6 +477,11 @@ class Diff:
 
     def backward(self, dl_dhdr_ptr: int, grad_ptr: int, stream: int = 0):
         check(lib().kt_diff_backward(self.handle, C.c_void_p(stream), C.c_void_p(dl_dhdr_ptr), C.c_void_p(grad_ptr)))
+
+    def backward_fp64(self, dl_dhdr_ptr: int, grad_ptr: int, stream: int = 0):
+        """The adjoint of the FP64 replay of the records (kt_diff_backward_fp64)."""
+        check(lib().kt_diff_backward_fp64(self.handle, C.c_void_p(stream), C.c_void_p(dl_dhdr_ptr),
+                                          C.c_void_p(grad_ptr)))
 
     def info(self) -> KtDiffInfo:
         i = KtDiffInfo()

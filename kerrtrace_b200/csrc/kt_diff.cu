@@ -599,13 +599,41 @@ __device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], 
     return t;
 }
 
+// Float records differentiated in double (the model that kt_diff_replay_fp64 evaluates): the
+// state and transmittance at the start of segment `target`, replayed in double from the ray's
+// double start through the recorded steps of the segments before it, in place of the float
+// checkpoint (which carries the float trajectory's rounding).  k and k7 are scratch.
+template <class R, class RR>
+__device__ __forceinline__ void replay_segment_start(const DiffRay& rr, const DiffRecRaw& rec, int target,
+                                                     const RayRun<R>& ry0, R a, R aa, R M, const Scene& sc,
+                                                     const DiffLut& dl, R (*k)[6], R* k7, R* s, R& tau) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) s[c] = ry0.s[c];
+    tau = R(1);
+    for (int si = rr.first_seg; si >= 0 && si != target; si = seg_at<RR>(rec, si)->next) {
+        const DiffSeg<RR>* sg = seg_at<RR>(rec, si);
+        for (int j = 0; j < sg->n; ++j) {
+            R nx[6];
+            dp5_stages<R>(s, (R)sg->h[j], ry0.pt, a, aa, M, k, nx, k7, false);
+            if (sg->hits >> j & 1u) {
+                R X[6], c3[3], al;
+                step_hit<R>(s, nx, k, k7, (R)sg->h[j], X, nullptr);
+                if (shade_eval<R, R>(X, ry0.pt, ry0.kt, sc, dl, c3, al)) tau *= R(1) - al;
+            }
+#pragma unroll
+            for (int c = 0; c < 6; ++c) s[c] = nx[c];
+        }
+    }
+}
+
 // Resident 128-thread blocks per SM asked of the compiler for the adjoint kernel: two, so that the
 // reverse sweep's dual-number right-hand sides keep their values in registers (225 registers,
 // no spills; four blocks per SM cap them at 128 with 452 B of spills and run 14% slower).
 template <class R> struct BackMinBlocks { static constexpr int v = 2; };
 template <> struct BackMinBlocks<double> { static constexpr int v = 2; };
 
-template <class R>
+// RR: the record type (float records of an FP32 object may be differentiated with R = double).
+template <class R, class RR = R>
 __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel(const Scene sc, const Camera cam, const CameraD camd,
                                                            const CameraD dcamd, const DiffRecRaw rec, const DiffLut dl,
                                                            const float4* __restrict__ dl_dhdr,
@@ -639,19 +667,69 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
             R TIN[kSegSteps];           // transmittance before a shaded crossing
             // the adjoint of the state is zero after the last shaded crossing: start there
             int si = rr.last_seg;
-            while (si >= 0 && seg_at<R>(rec, si)->hits == 0u) si = seg_at<R>(rec, si)->prev;
+            while (si >= 0 && seg_at<RR>(rec, si)->hits == 0u) si = seg_at<RR>(rec, si)->prev;
+            // float records in double: one replay from the ray's start gives the start states of
+            // the segments up to si (the last kStoredStarts of them kept; earlier ones, on rays
+            // longer than that, are replayed again when their turn comes)
+            constexpr int kStoredStarts = std::is_same<R, RR>::value ? 1 : 8;
+            R SS[kStoredStarts][6], ST[kStoredStarts];
+            int SID[kStoredStarts];
+            if constexpr (!std::is_same<R, RR>::value) {
+#pragma unroll
+                for (int q = 0; q < kStoredStarts; ++q) SID[q] = -1;
+                R s[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) s[c] = ry0.s[c];
+                R tau = R(1);
+                int ord = 0;
+                for (int sj = rr.first_seg; sj >= 0; sj = seg_at<RR>(rec, sj)->next, ++ord) {
+                    const int q = ord % kStoredStarts;
+                    SID[q] = sj;
+                    ST[q] = tau;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) SS[q][c] = s[c];
+                    if (sj == si) break;
+                    const DiffSeg<RR>* sg = seg_at<RR>(rec, sj);
+                    for (int j = 0; j < sg->n; ++j) {
+                        R nx[6];
+                        dp5_stages<R>(s, (R)sg->h[j], pt, a, aa, M, K[0], nx, K7, false);
+                        if (sg->hits >> j & 1u) {
+                            R X[6], c3[3], al;
+                            step_hit<R>(s, nx, K[0], K7, (R)sg->h[j], X, nullptr);
+                            if (shade_eval<R, R>(X, pt, kt, sc, dl, c3, al)) tau *= R(1) - al;
+                        }
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) s[c] = nx[c];
+                    }
+                }
+            }
             bool first = true;
             while (si >= 0) {
-                const DiffSeg<R>* sg = seg_at<R>(rec, si);
+                const DiffSeg<RR>* sg = seg_at<RR>(rec, si);
                 const unsigned hits = sg->hits;
                 const int n = first ? 32 - __clz((int)hits) : sg->n;
                 first = false;
                 // forward sweep: states, stages, transmittance at the shaded crossings
                 {
                     R s[6];
+                    R tau;
+                    if constexpr (std::is_same<R, RR>::value) {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) s[c] = sg->s[c];
-                    R tau = sg->tau;
+                        for (int c = 0; c < 6; ++c) s[c] = sg->s[c];
+                        tau = sg->tau;
+                    } else {
+                        int q = -1;
+#pragma unroll
+                        for (int i = 0; i < kStoredStarts; ++i)
+                            if (SID[i] == si) q = i;
+                        if (q >= 0) {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) s[c] = SS[q][c];
+                            tau = ST[q];
+                        } else {
+                            replay_segment_start<R, RR>(rr, rec, si, ry0, a, aa, M, sc, dl, K[0], K7, s, tau);
+                        }
+                    }
                     for (int j = 0; j < n; ++j) {
                         R nx[6];
 #pragma unroll
@@ -828,18 +906,21 @@ cudaError_t launch_diff_forward(const Scene& sc, const Camera& cam, const Camera
 
 cudaError_t launch_diff_backward(const Scene& sc, const Camera& cam, const CameraD& camd, const CameraD& dcamd,
                                  const DiffRecRaw& rec, const DiffLut& dl, const float4* dl_dhdr, double* grad,
-                                 const DiffWork& wk, cudaStream_t st) {
+                                 const DiffWork& wk, cudaStream_t st, bool float_records) {
     const unsigned n = (unsigned)sc.width * (unsigned)sc.height;
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(wk.ctl, 0, (2 * kWorkBuckets + 1) * sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
     const dim3 g256((n + 255) / 256), g128((n + 127) / 128);
-    if (sc.precision == 2) diff_bucket_kernel<double><<<g256, 256, 0, st>>>(sc, rec, dl_dhdr, wk.bucket, wk.ctl);
+    if (sc.precision == 2 && !float_records) diff_bucket_kernel<double><<<g256, 256, 0, st>>>(sc, rec, dl_dhdr, wk.bucket, wk.ctl);
     else diff_bucket_kernel<float><<<g256, 256, 0, st>>>(sc, rec, dl_dhdr, wk.bucket, wk.ctl);
     diff_bucket_scan_kernel<<<1, 32, 0, st>>>(wk.ctl);
     diff_bucket_scatter_kernel<<<g256, 256, 0, st>>>(n, wk.bucket, wk.ctl, wk.order);
     const unsigned* n_work = wk.ctl + 2 * kWorkBuckets;
-    if (sc.precision == 2)
+    if (sc.precision == 2 && float_records)
+        diff_backward_kernel<double, float><<<g128, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, wk.order,
+                                                                  n_work);
+    else if (sc.precision == 2)
         diff_backward_kernel<double><<<g128, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, wk.order, n_work);
     else
         diff_backward_kernel<float><<<g128, 128, 0, st>>>(sc, cam, camd, dcamd, rec, dl, dl_dhdr, grad, wk.order, n_work);

@@ -90,8 +90,10 @@ struct DiffWork {
 // Adjoint: grad[0..3] += d(sum_p dl_dhdr[p] . hdr[p]) / d(spin, inclination in degrees,
 // temperature-scale parameter, disk outer radius).  dcamd = d(camera)/d(inclination in degrees).
 // The float path starts its rays from cam (the renderer's camera), the double path from camd.
+// float_records (double arithmetic only): the records are DiffSeg<float>, differentiated as the
+// FP64 replay of their steps (segment starts replayed in double from the ray's start).
 cudaError_t launch_diff_backward(const Scene& sc, const Camera& cam, const CameraD& camd, const CameraD& dcamd,
                                  const DiffRecRaw& rec, const DiffLut& dl, const float4* dl_dhdr, double* grad,
-                                 const DiffWork& work, cudaStream_t stream);
+                                 const DiffWork& work, cudaStream_t stream, bool float_records = false);
 
 }  // namespace ktd

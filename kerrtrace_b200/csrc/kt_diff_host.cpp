@@ -182,6 +182,7 @@ struct kt_diff {
     ktd::Camera cam_rec{};
     ktd::CameraD camd_rec{}, dcamd_rec{};
     ktd::DiffLut dl_rec{};
+    kt_diff_params theta_rec{};
 };
 
 namespace {
@@ -383,6 +384,7 @@ kt_status kt_diff_forward(kt_diff* d, void* stream, const kt_diff_params* theta,
     d->camd_rec = camd;
     d->dcamd_rec = dcamd;
     d->dl_rec = dl;
+    d->theta_rec = *theta;
     return KT_OK;
 }
 
@@ -435,6 +437,29 @@ kt_status kt_diff_backward(kt_diff* d, void* stream, const float* dl_dhdr, doubl
     e = ktd::launch_diff_backward(d->sc_rec, d->cam_rec, d->camd_rec, d->dcamd_rec, record_of(d), d->dl_rec,
                                   reinterpret_cast<const float4*>(dl_dhdr), grad_out, d->work, st);
     if (e != cudaSuccess) return err_cuda(e, "diff backward launch");
+    return KT_OK;
+}
+
+kt_status kt_diff_backward_fp64(kt_diff* d, void* stream, const float* dl_dhdr, double* grad_out) {
+    if (!d || !dl_dhdr || !grad_out) return err_arg("NULL argument");
+    if (!d->have_record) return ktd::set_error(KT_ERR_NOT_READY, "kt_diff_backward_fp64 needs a kt_diff_forward first");
+    if (d->cfg.precision != KT_PREC_FP32) return kt_diff_backward(d, stream, dl_dhdr, grad_out);
+    DevGuard g(d->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    ktd::Scene sc;
+    ktd::Camera cam;
+    ktd::CameraD camd, dcamd;
+    ktd::DiffLut dl;
+    // the recorded point in double: double theta, camera and disk table (uploaded into the
+    // replay's tables, like kt_diff_replay_fp64)
+    kt_status s = prepare(d, &d->theta_rec, d->lut_rep, st, &sc, &cam, &camd, &dcamd, &dl, true);
+    if (s != KT_OK) return s;
+    sc.max_attempts = 1;
+    cudaError_t e = cudaMemsetAsync(grad_out, 0, 4 * sizeof(double), st);
+    if (e != cudaSuccess) return err_cuda(e, "gradient reset");
+    e = ktd::launch_diff_backward(sc, cam, camd, dcamd, record_of(d), dl, reinterpret_cast<const float4*>(dl_dhdr),
+                                  grad_out, d->work, st, true);
+    if (e != cudaSuccess) return err_cuda(e, "diff FP64 backward launch");
     return KT_OK;
 }
 

@@ -173,6 +173,40 @@ def test_fp32_adjoint_matches_central_differences_of_its_model(cuda):
     d.close()
 
 
+def backward_fp64(torch, d, w):
+    g = torch.zeros(4, dtype=torch.float64, device="cuda")
+    d.backward_fp64(w.data_ptr(), g.data_ptr())
+    torch.cuda.synchronize()
+    return g.cpu().numpy()
+
+
+def test_fp64_adjoint_of_fp32_records_matches_central_differences(cuda):
+    """kt_diff_backward_fp64 on an FP32 object differentiates its records replayed in double
+    (the model of kt_diff_replay_fp64), segment starts included: the loss gradient matches that
+    model's central differences to 1e-4 in all four parameters, r_out included, where the FP32
+    adjoint carries the float rounding of its hit states."""
+    _, _, d = make(kt.PREC_FP32)
+    hdr = forward(cuda, d, THETA)
+    fd, mask = central_differences(cuda, d, replay_fp64)
+    lit = hdr[:, :3].sum(1) > 0
+    assert int(mask.sum()) <= 0.02 * int(lit.sum())
+    n = SIZE * SIZE
+    rng = np.random.default_rng(1)
+    w = cuda.tensor((rng.standard_normal((n, 4)) + 1.0).astype(np.float32), device="cuda")
+    w[:, 3] = 0
+    w[mask] = 0
+    g64 = backward_fp64(cuda, d, w)
+    g32 = backward(cuda, d, w)
+    for j in range(4):
+        ref = float((fd[j] * w[:, :3].double()).sum())
+        print(NAMES[j], g64[j], g32[j], ref, abs(g64[j] - ref) / abs(ref))
+        assert abs(g64[j] - ref) <= 1e-4 * abs(ref), (NAMES[j], g64[j], ref)
+    # and the FP32 adjoint of the same records is close to it where it is accurate
+    for j in range(3):
+        assert abs(g32[j] - g64[j]) <= 1e-3 * abs(g64[j]), NAMES[j]
+    d.close()
+
+
 def test_fp32_adjoint_tracks_fp64(cuda):
     n = SIZE * SIZE
     rng = np.random.default_rng(4)
