@@ -600,9 +600,25 @@ __device__ __forceinline__ R step_hit(const R* s, const R* nx, const R (*k)[6], 
 }
 
 // Float records differentiated in double (the model that kt_diff_replay_fp64 evaluates): the
-// state and transmittance at the start of segment `target`, replayed in double from the ray's
-// double start through the recorded steps of the segments before it, in place of the float
-// checkpoint (which carries the float trajectory's rounding).  k and k7 are scratch.
+// float checkpoints carry the float trajectory's rounding, so segment starts are replayed in
+// double from the ray's double start instead.  sweep_segment advances the state s and the
+// transmittance tau through every recorded step of one segment; k and k7 are scratch.
+template <class R, class RR>
+__device__ __forceinline__ void sweep_segment(const DiffSeg<RR>* sg, R pt, R kt, R a, R aa, R M, const Scene& sc,
+                                              const DiffLut& dl, R (*k)[6], R* k7, R* s, R& tau) {
+    for (int j = 0; j < sg->n; ++j) {
+        R nx[6];
+        dp5_stages<R>(s, (R)sg->h[j], pt, a, aa, M, k, nx, k7, false);
+        if (sg->hits >> j & 1u) {
+            R X[6], c3[3], al;
+            step_hit<R>(s, nx, k, k7, (R)sg->h[j], X, nullptr);
+            if (shade_eval<R, R>(X, pt, kt, sc, dl, c3, al)) tau *= R(1) - al;
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) s[c] = nx[c];
+    }
+}
+// The state and transmittance at the start of segment `target`, replayed from the ray's start.
 template <class R, class RR>
 __device__ __forceinline__ void replay_segment_start(const DiffRay& rr, const DiffRecRaw& rec, int target,
                                                      const RayRun<R>& ry0, R a, R aa, R M, const Scene& sc,
@@ -610,20 +626,8 @@ __device__ __forceinline__ void replay_segment_start(const DiffRay& rr, const Di
 #pragma unroll
     for (int c = 0; c < 6; ++c) s[c] = ry0.s[c];
     tau = R(1);
-    for (int si = rr.first_seg; si >= 0 && si != target; si = seg_at<RR>(rec, si)->next) {
-        const DiffSeg<RR>* sg = seg_at<RR>(rec, si);
-        for (int j = 0; j < sg->n; ++j) {
-            R nx[6];
-            dp5_stages<R>(s, (R)sg->h[j], ry0.pt, a, aa, M, k, nx, k7, false);
-            if (sg->hits >> j & 1u) {
-                R X[6], c3[3], al;
-                step_hit<R>(s, nx, k, k7, (R)sg->h[j], X, nullptr);
-                if (shade_eval<R, R>(X, ry0.pt, ry0.kt, sc, dl, c3, al)) tau *= R(1) - al;
-            }
-#pragma unroll
-            for (int c = 0; c < 6; ++c) s[c] = nx[c];
-        }
-    }
+    for (int si = rr.first_seg; si >= 0 && si != target; si = seg_at<RR>(rec, si)->next)
+        sweep_segment<R, RR>(seg_at<RR>(rec, si), ry0.pt, ry0.kt, a, aa, M, sc, dl, k, k7, s, tau);
 }
 
 // Resident 128-thread blocks per SM asked of the compiler for the adjoint kernel: two, so that the
@@ -689,18 +693,7 @@ __global__ void __launch_bounds__(128, BackMinBlocks<R>::v) diff_backward_kernel
 #pragma unroll
                     for (int c = 0; c < 6; ++c) SS[q][c] = s[c];
                     if (sj == si) break;
-                    const DiffSeg<RR>* sg = seg_at<RR>(rec, sj);
-                    for (int j = 0; j < sg->n; ++j) {
-                        R nx[6];
-                        dp5_stages<R>(s, (R)sg->h[j], pt, a, aa, M, K[0], nx, K7, false);
-                        if (sg->hits >> j & 1u) {
-                            R X[6], c3[3], al;
-                            step_hit<R>(s, nx, K[0], K7, (R)sg->h[j], X, nullptr);
-                            if (shade_eval<R, R>(X, pt, kt, sc, dl, c3, al)) tau *= R(1) - al;
-                        }
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) s[c] = nx[c];
-                    }
+                    sweep_segment<R, RR>(seg_at<RR>(rec, sj), pt, kt, a, aa, M, sc, dl, K[0], K7, s, tau);
                 }
             }
             bool first = true;
