@@ -219,6 +219,15 @@ def test_diff_rejects_unsupported_configurations(kt):
             kt.Diff(c, view)
 
 
+def test_diff_entry_points_refuse_null_arguments(kt):
+    """The adjoint entry points check their arguments on the host, before any device work."""
+    L = kt.lib()
+    g = (C.c_double * 4)()
+    for fn in (L.kt_diff_backward, L.kt_diff_backward_fp64):
+        assert fn(None, None, None, None) == kt.KT_ERR_INVALID_ARG
+        assert fn(None, None, C.cast(g, C.c_void_p), C.cast(g, C.c_void_p)) == kt.KT_ERR_INVALID_ARG
+
+
 def _struct_bytes(s) -> bytes:
     return bytes(C.string_at(C.addressof(s), C.sizeof(s)))
 
