@@ -32,7 +32,8 @@ def _hdr_input(torch, cfg, seed):
 @pytest.mark.parametrize("name,size,radius", [("t1", None, None), ("t2", None, None), ("c2", (333, 190), None),
                                               ("c2", (64, 40), 48.0), ("t1", (50, 70), 0.0),
                                               ("c2", (96, 300), 70.0), ("c2", (72, 260), 95.0),
-                                              ("c2", (80, 90), 100.0), ("t1", (1, 1), None)])
+                                              ("c2", (80, 90), 100.0), ("t1", (1, 1), None),
+                                              ("c2", (1920, 1080), None)])
 def test_post_bit_identical_to_reference(cuda, orc, name, size, radius):
     cfg, _ = workloads.scene(name)
     if size:
