@@ -200,6 +200,22 @@ def test_large_frame_matches_reference_kernel(cuda):
     assert np.array_equal(err_o, err_r)
 
 
+def test_benchmark_frame_matches_reference_kernel(cuda):
+    """The benchmark's own frame (the 1080p scene at 1920 x 1080) in the launch shape the
+    autotuner installs for it, against the reference's trace_kernel: every HDR pixel and the
+    error word bit-identical."""
+    import ctypes as C
+    cfg, cam = workloads.scene("c2")
+    ctx = kt.Context(cfg)
+    kt.check(kt.lib().kt_context_autotune(ctx.handle, None, C.byref(cam), 2, None, 0, None, None))
+    ours, err_o, _, _ = run_ours(cuda, cfg, cam, kt.SCHED_AUTO, ctx=ctx)
+    ctx.close()
+    ref, err_r = run_ref(cuda, "c2", cfg, cam)
+    diff = np.flatnonzero((ours.view(np.uint32) != ref.view(np.uint32)).any(1))
+    assert len(diff) == 0, diff[:10]
+    assert np.array_equal(err_o, err_r)
+
+
 def test_c1_full_frame_matches_reference_kernel(cuda):
     """The plain-method benchmark scene at its full 256 x 256 (tolerance 1e-8, a = 0.9) against
     the reference's trace_kernel on the same inputs."""
