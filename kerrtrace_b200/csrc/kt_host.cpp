@@ -950,7 +950,6 @@ kt_status kt_post_fused(kt_context* ctx, void* stream, const float* hdr, uint32_
 // =========================================================================================
 struct kt_frame {
     float* hdr = nullptr;
-    float* bloom = nullptr;
     uint32_t* image = nullptr;
     uint32_t* host_image = nullptr;  // pinned
     uint32_t* err = nullptr;
@@ -966,8 +965,8 @@ struct kt_frame {
 // post-processed on a non-blocking stream of the highest priority and come back to pinned memory
 // on a non-blocking copy stream.  With two frames in flight the post passes of one frame run
 // while the next frame is traced: their blocks are dispatched ahead of the trace's remaining
-// blocks as SMs free up, and being latency-bound they fill issue slots that the FMA-bound trace
-// leaves.  The copy of one frame overlaps the trace of the next as well.
+// blocks as SMs free up, so part of their time overlaps the next trace.  The copy of one frame
+// overlaps the trace of the next as well.  The post passes use the context's bloom buffer.
 struct kt_renderer {
     kt_context* ctx = nullptr;
     cudaStream_t stream = nullptr;   // the legacy default stream, like cudarc's default_stream()
@@ -987,7 +986,6 @@ void destroy_renderer(kt_renderer* r) {
         cudaDeviceSynchronize();
         for (auto& f : r->frames) {
             cudaFree(f.hdr);
-            cudaFree(f.bloom);
             cudaFree(f.image);
             cudaFree(f.err);
             cudaFreeHost(f.host_image);
@@ -1032,7 +1030,6 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
     for (auto& f : r->frames) {
         cudaError_t e;
         if ((e = cudaMalloc(&f.hdr, px * 4 * sizeof(float))) != cudaSuccess ||
-            (e = cudaMalloc(&f.bloom, px * 4 * sizeof(float))) != cudaSuccess ||
             (e = cudaMalloc(&f.image, px * sizeof(uint32_t))) != cudaSuccess ||
             (e = cudaMalloc(&f.err, 2 * sizeof(uint32_t))) != cudaSuccess ||
             (e = cudaMallocHost(&f.host_image, px * sizeof(uint32_t))) != cudaSuccess ||
@@ -1041,7 +1038,6 @@ kt_status kt_renderer_new(const kt_config* cfg, int device, kt_renderer** out) {
             (e = cudaEventCreateWithFlags(&f.computed, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&f.traced, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaMemset(f.hdr, 0, px * 4 * sizeof(float))) != cudaSuccess ||
-            (e = cudaMemset(f.bloom, 0, px * 4 * sizeof(float))) != cudaSuccess ||
             (e = cudaMemset(f.image, 0, px * sizeof(uint32_t))) != cudaSuccess ||
             (e = cudaMemset(f.err, 0, 2 * sizeof(uint32_t))) != cudaSuccess) {
             st = cuda_fail(e, "allocate frame buffers");
